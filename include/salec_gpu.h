@@ -1,0 +1,151 @@
+/*
+ * salec_gpu.h - C ABI of the B200 (sm_100a) per-timestep mesh update of SALEc2d.
+ *
+ * The reference has no plugin or FFI layer: its step is a sequence of
+ * `void f(sale2d_var *, node_type, double dt)` sweeps called from the time loop in
+ * src/salec2d.c:115-272 (declarations in src/sale2d.h:397-466, src/strength.h:11-35,
+ * src/ejecta.h:35-36, src/tracer.h:16-24). These entry points replace that loop body:
+ * a host driver keeps the reference's own initialisation (deck parser, EOS loaders,
+ * target profile, geometry) and output writers, uploads the initialised fields once,
+ * calls salec_gpu_step() per cycle, and downloads fields at output cycles.
+ *
+ * Conventions (kept from the reference's interface):
+ *   - field data crosses the boundary in the reference's own memory layout: one block per
+ *     field, points with the x index fastest (src/mpi_vec/mpi_vec.h:372-376), and the
+ *     components of one point contiguous, exactly the bytes of field_var.data;
+ *   - point counts include the two-cell pad: cells (nx+4) x (ny+4), vertices (nx+5) x (ny+5),
+ *     x faces (nx+5) x (ny+4), y faces (nx+4) x (ny+5) (src/sale2d_back.c:169-175);
+ *   - the caller owns every host buffer; the library owns every device buffer.
+ * Unlike the reference (which calls exit(0) on errors, e.g. src/sale2d_back.c:49-51), every
+ * entry point returns SALEC_OK or a negative salec_status and never terminates the process.
+ * One handle is used by one host thread at a time; all its work runs on one CUDA stream.
+ */
+#ifndef SALEC_GPU_H
+#define SALEC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct salec_gpu salec_gpu;
+
+enum salec_status {
+    SALEC_OK = 0,
+    SALEC_ERR_ARG = -1,         /* invalid argument, unknown name or size mismatch */
+    SALEC_ERR_CUDA = -2,        /* a CUDA runtime call failed; see salec_gpu_last_error() */
+    SALEC_ERR_ALLOC = -3,       /* device or host allocation failed */
+    SALEC_ERR_STATE = -4,       /* call not valid in the handle's current state */
+    SALEC_ERR_UNSUPPORTED = -5, /* option the reference supports but this build does not */
+    SALEC_ERR_NUMERIC = -6      /* non-finite values detected by salec_gpu_check() */
+};
+
+/* Equation-of-state kinds, numbered as the reference's eos_type (src/eos/eos_state.h:222-228). */
+enum salec_eos_kind { SALEC_EOS_ANEOS = 0, SALEC_EOS_TILLOTSON = 1, SALEC_EOS_ANEOS_SIEDEN = 2 };
+
+/* Damping layer kinds, numbered as the reference's damp_type_t (src/sale2d.h:252-260). */
+enum salec_damp_kind { SALEC_DAMP_PML = 0, SALEC_DAMP_PML2 = 1, SALEC_DAMP_PML3 = 2,
+                       SALEC_DAMP_SBC = 3, SALEC_DAMP_CTLG = 4, SALEC_DAMP_NONE = 5 };
+
+/* Strength, damage, tensile and porosity functions, in the order of the reference's
+ * registry str_func_list (src/strength.c:860-875); the name lookup is salec_gpu_func_index(). */
+enum salec_func {
+    SALEC_FN_SIMPLE_ROCK = 0, SALEC_FN_SIMPLE_SHEAR = 1, SALEC_FN_JOHNSON_COOK1 = 2,
+    SALEC_FN_JOHNSON_COOK2 = 3, SALEC_FN_ROCK_STRENGTH_T = 4, SALEC_FN_ICE_STRENGTH = 5,
+    SALEC_FN_COLLINS = 6, SALEC_FN_IVANOV = 7, SALEC_FN_SIMPLE_TENSILE = 8, SALEC_FN_NONE = 9,
+    SALEC_FN_WUNNEMANN = 10, SALEC_FN_VON_MISES1 = 11, SALEC_FN_VON_MISES2 = 12
+};
+
+/*
+ * Run-wide parameters. Each field is the value the reference holds after initialisation,
+ * in sale2d_var (src/sale2d.h:34-174), mesh2d_info (:319-386) or cycle_control (:176-208).
+ * go[4] are the ghost options of the left, right, bottom and top boundaries after
+ * boundary_str2opt and the Ox < 1e-6 mirror rule (src/sale2d_back.c:230-238, :405-428),
+ * numbered as the reference's ght_opt (src/mpi_vec/mpi_vec_types.h:74-95).
+ */
+typedef struct salec_run_desc {
+    int nx, ny;                 /* interior cells (mesh.npx, mesh.npy) of the single domain */
+    int nmat;                   /* materials including vacuum (material.nm) */
+    int damp_type;              /* salec_damp_kind */
+    int go[4];
+    int partpres, porosity_model, acoustic_fluid, tensile_failure;
+    int tracer_lubrication, tracer_lub_gy0, tracer_lub_gy1;
+    double avis1, avis2, anc;
+    double density_cutoff, velocity_max, velocity_min, acceleration_min;
+    double alpha_damp_x, alpha_damp_y, damp_time;
+    double threshold_z, flow_resistance, flow_friction;
+    double tracer_lub_y0, tracer_lub_frac;
+    double max_dt, dt, time;    /* cycle.maxdt, current dt and simulated time */
+    int i_step;
+} salec_run_desc;
+
+/*
+ * One material (index >= 1; index 0 is vacuum and is ignored): the reference's
+ * state_reference (src/eos/eos_state.h:43-151) plus its EOS table. Table arrays are read
+ * during salec_gpu_create() only.
+ */
+typedef struct salec_material_desc {
+    int eos_type;               /* salec_eos_kind */
+    int yfunc, tfunc, dsdf, porfunc;   /* salec_func for shear strength, tensile strength,
+                                          damage increment and porosity increment */
+    double VaporDen, MeltDen, GaCoef;
+    double Yint0, Yfricint, Ylimint, Ydam0, Yfricdam, Ylimdam, Yten0;
+    double IvanA, IvanB, IvanC, Pbd, Pbp, minPint, minPdam;
+    double JCA, JCB, JCN, JCC, JCM, JCTREF, JCMaxPlastic;
+    double Asimon, Csimon, Tmelt0, Tfrac, Tdelta;
+    int PolyLiq, PolySol;
+    double Tlidc1, Tlidc2, Tlidc3, Tsolc1, Tsolc2, Tsolc3;
+    double Toff, Cvib, VibMax, Tdamp, Pvlim, Acvis;
+    double alpha0, alphax, epse0, chi, kappa, avel, epsec, epsex, alphamax, alphamax2, alphae;
+    double gamfrac, melt_viscosity;
+    /* Tillotson: Rho0, Cv, A, B, E0, a, b, Alpha, Beta, Eiv, Ecv, Tref, StepDen
+       (src/eos/eos_state.h:168-186) and the cold-energy curve of TillColdEnergy. */
+    double till[13];
+    int cold_n;
+    const double *cold_xden, *cold_yeng;
+    /* Tabulated kinds: axes and Data[iT][iD][0..2] flattened as [ntem][nden][3]. */
+    int ntem, nden;
+    const double *xtem, *yden, *data;
+} salec_material_desc;
+
+/* Create a handle on the current CUDA device. mats has nmat entries (entry 0 unused). */
+int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats, salec_gpu **out);
+int salec_gpu_destroy(salec_gpu *h);
+
+/* Field names are the reference's member names of sale2d_var (e.g. "m_vof", "v_vel",
+ * "bx_phi", "y_profile"). Returns the field index or -1. */
+int salec_gpu_field_index(const char *name);
+/* Points in x and y and doubles per point of a field in the reference's layout. */
+int salec_gpu_field_shape(const salec_gpu *h, int field, int *nx, int *ny, int *ncomp);
+/* Copy a whole field from / to a host buffer of n doubles in the reference's layout. */
+int salec_gpu_set_field(salec_gpu *h, int field, const double *host, long long n);
+int salec_gpu_get_field(salec_gpu *h, int field, double *host, long long n);
+
+/* Advance nsteps full cycles: the loop body of src/salec2d.c:115-272 without the output point. */
+int salec_gpu_step(salec_gpu *h, int nsteps);
+/* Run phases first..last of one cycle (numbering of oracle/ref_driver.c); for stepwise checks. */
+int salec_gpu_phases(salec_gpu *h, int first, int last);
+/* Block until the handle's stream is idle. */
+int salec_gpu_sync(salec_gpu *h);
+
+/* Scalars: "dt", "time", "i_step", "damp_time", "max_dt". */
+int salec_gpu_get_scalar(salec_gpu *h, const char *name, double *value);
+int salec_gpu_set_scalar(salec_gpu *h, const char *name, double value);
+
+/* Lagrangian tracers (src/tracer.c:52-175). Rows of 12 doubles per tracer:
+ * x, y, vx, vy, mpre, mtem, gx, gy, tag, matid, cell_x, cell_y. get returns live tracers in
+ * their original order; *n is in/out (capacity in, count out). */
+int salec_gpu_set_tracers(salec_gpu *h, int n, const double *rows);
+int salec_gpu_get_tracers(salec_gpu *h, double *rows, int *n);
+
+/* Count non-finite values in the evolving cell and vertex fields; SALEC_ERR_NUMERIC if any. */
+int salec_gpu_check(salec_gpu *h, long long *n_bad);
+
+/* Strength/damage/porosity function index for a reference name (case-insensitive), or -1. */
+int salec_gpu_func_index(const char *name);
+/* Message of the last error on this thread. */
+const char *salec_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

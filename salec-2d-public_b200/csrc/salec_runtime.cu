@@ -1,0 +1,626 @@
+// Host runtime of the B200 mesh update: device memory of one simulation, upload/download in
+// the reference's layout, the launch sequence of one cycle, and the C ABI of salec_gpu.h.
+#include "../../include/salec_gpu.h"
+#include "salec_device.cuh"
+#include "salec_kernels.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace salec;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (expr);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(SALEC_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------------ field table
+namespace {
+
+enum Loc { L_CELL, L_VERT, L_BX, L_BY, L_COL };
+enum NC { NC_FIX, NC_MAT, NC_PHI };
+
+struct FieldInfo {
+    const char *name;
+    Loc loc;
+    NC nck;
+    int n;
+    size_t off;   // offset of the pointer inside salec::Fields
+};
+
+#define F_(name, loc, nck, n) {#name, loc, nck, n, offsetof(Fields, name)}
+const FieldInfo kFields[] = {
+    F_(v_vel, L_VERT, NC_FIX, 2), F_(v_bf, L_VERT, NC_FIX, 2), F_(v_acc, L_VERT, NC_FIX, 2),
+    F_(v_dis, L_VERT, NC_FIX, 2), F_(v_pos, L_VERT, NC_FIX, 2), F_(v_vof, L_VERT, NC_MAT, 1),
+    F_(v_mass, L_VERT, NC_FIX, 2), F_(v_vol, L_VERT, NC_FIX, 5), F_(v_subvol, L_VERT, NC_FIX, 4),
+    F_(v_laplace, L_VERT, NC_FIX, 9), F_(v_suf, L_VERT, NC_FIX, 8), F_(v_alpha, L_VERT, NC_FIX, 2),
+    F_(v_beta, L_VERT, NC_FIX, 2),
+    F_(e_vel, L_CELL, NC_FIX, 2), F_(e_div_vel, L_CELL, NC_FIX, 1), F_(e_grad_vel, L_CELL, NC_FIX, 5),
+    F_(e_ste, L_CELL, NC_FIX, 4), F_(e_mu, L_CELL, NC_FIX, 1), F_(e_dvel, L_CELL, NC_FIX, 2),
+    F_(e_pre, L_CELL, NC_FIX, 1), F_(e_tem, L_CELL, NC_FIX, 1), F_(e_den, L_CELL, NC_FIX, 1),
+    F_(e_eng, L_CELL, NC_FIX, 1), F_(e_csd, L_CELL, NC_FIX, 1), F_(e_dam, L_CELL, NC_FIX, 1),
+    F_(e_cvs, L_CELL, NC_FIX, 1), F_(m_vof, L_CELL, NC_MAT, 1), F_(m_den, L_CELL, NC_MAT, 1),
+    F_(m_eng, L_CELL, NC_MAT, 1), F_(m_pty, L_CELL, NC_MAT, 1), F_(e_wpt, L_CELL, NC_FIX, 4),
+    F_(e_pos, L_CELL, NC_FIX, 4), F_(e_vol, L_CELL, NC_FIX, 1), F_(e_suf, L_CELL, NC_FIX, 8),
+    F_(e_grad, L_CELL, NC_FIX, 12), F_(e_subvol, L_CELL, NC_FIX, 8), F_(e_q, L_CELL, NC_FIX, 1),
+    F_(e_strength, L_CELL, NC_FIX, 1), F_(e_cnd, L_CELL, NC_FIX, 1), F_(e_tps, L_CELL, NC_FIX, 1),
+    F_(e_ste2s, L_CELL, NC_FIX, 1), F_(e_sta2s, L_CELL, NC_FIX, 1), F_(e_alpha, L_CELL, NC_FIX, 2),
+    F_(e_beta, L_CELL, NC_FIX, 4), F_(e_sigma, L_CELL, NC_FIX, 2), F_(e_dampref, L_CELL, NC_FIX, 3),
+    F_(e_vib, L_CELL, NC_FIX, 1), F_(e_ejt, L_CELL, NC_FIX, 1),
+    F_(bx_phi, L_BX, NC_PHI, 1), F_(by_phi, L_BY, NC_PHI, 1), F_(bx_normal, L_BX, NC_FIX, 2),
+    F_(by_normal, L_BY, NC_FIX, 2), F_(y_profile, L_COL, NC_FIX, 1),
+};
+#undef F_
+constexpr int kNumFields = sizeof(kFields) / sizeof(kFields[0]);
+
+int field_by_name(const char *n)
+{
+    if (!n) return -1;
+    for (int k = 0; k < kNumFields; ++k)
+        if (strcmp(kFields[k].name, n) == 0) return k;
+    // the reference's e_vof is the same array as m_vof (src/sale2d.c:333)
+    if (strcmp(n, "e_vof") == 0) return field_by_name("m_vof");
+    return -1;
+}
+
+const char *kFuncNames[] = {"SimpleRock", "SimpleShear", "JohnsonCook1", "JohnsonCook2", "RockStrengthT",
+                            "IceStrength", "Collins", "Ivanov", "SimpleTensile", "None", "Wunnemann",
+                            "VonMises1", "VonMises2"};
+
+struct Gather {
+    GatherBatch batch{};
+    bool two_pass = false;
+    int ncomp_max = 0;
+};
+
+} // namespace
+
+struct salec_gpu {
+    Dims d{};
+    RunParams rp{};
+    int go[4] = {0, 0, 0, 0};
+    cudaStream_t stream = nullptr;
+    double *pool = nullptr;
+    size_t pool_doubles = 0;
+    Fields f{};
+    DevMat *mat = nullptr;
+    std::vector<void *> owned;   // device allocations besides the pool
+    Scal *scal = nullptr;
+    Scal *scal_host = nullptr;   // pinned mirror
+    double *scratch = nullptr;   // gather scratch
+    size_t scratch_doubles = 0;
+    double *staging = nullptr;   // AoS staging for field transfer
+    size_t staging_doubles = 0;
+    Gather g_mvof, g_dvel_den, g_evel, g_pre_ste_q, g_flux_state, r_vel, r_acc, r_dis;
+    int ntracer = 0;
+
+    Ctx ctx() const
+    {
+        Ctx c;
+        c.d = d;
+        c.f = f;
+        c.rp = rp;
+        c.mat = mat;
+        c.scal = scal;
+        return c;
+    }
+};
+
+namespace {
+
+int field_ncomp(const salec_gpu *h, int k)
+{
+    const FieldInfo &fi = kFields[k];
+    if (fi.nck == NC_MAT) return h->d.nmat * fi.n;
+    if (fi.nck == NC_PHI) return h->d.phi;
+    return fi.n;
+}
+
+void field_points(const salec_gpu *h, int k, int &nx, int &ny)
+{
+    switch (kFields[k].loc) {
+    case L_CELL: nx = h->d.enx; ny = h->d.eny; break;
+    case L_VERT: nx = h->d.vnx; ny = h->d.vny; break;
+    case L_BX: nx = h->d.vnx; ny = h->d.eny; break;
+    case L_BY: nx = h->d.enx; ny = h->d.vny; break;
+    default: nx = h->d.enx; ny = 1; break;
+    }
+}
+
+double *&field_ptr(salec_gpu *h, int k)
+{
+    return *reinterpret_cast<double **>(reinterpret_cast<char *>(&h->f) + kFields[k].off);
+}
+
+template <typename T>
+int upload_vec(salec_gpu *h, const std::vector<T> &v, const T **out)
+{
+    if (v.empty()) { *out = nullptr; return SALEC_OK; }
+    void *p = nullptr;
+    CUDA_TRY(cudaMalloc(&p, v.size() * sizeof(T)));
+    h->owned.push_back(p);
+    CUDA_TRY(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    *out = static_cast<const T *>(p);
+    return SALEC_OK;
+}
+
+int make_gather(salec_gpu *h, Gather &g, const std::vector<std::pair<int, GatherMap>> &maps)
+{
+    g = Gather();
+    g.batch.nfield = (int)maps.size();
+    int total = 0;
+    for (size_t k = 0; k < maps.size(); ++k) g.ncomp_max = std::max(g.ncomp_max, field_ncomp(h, maps[k].first));
+    for (size_t k = 0; k < maps.size(); ++k) {
+        const int fid = maps[k].first;
+        const GatherMap &m = maps[k].second;
+        GatherField &gf = g.batch.field[k];
+        gf.base = field_ptr(h, fid);
+        gf.plane = h->d.PL;
+        gf.ncomp = field_ncomp(h, fid);
+        gf.ncomp_max = g.ncomp_max;
+        int rc = upload_vec(h, m.dst, &gf.dst);
+        if (rc) return rc;
+        rc = upload_vec(h, m.src, &gf.src);
+        if (rc) return rc;
+        rc = upload_vec(h, m.ops, &gf.ops);
+        if (rc) return rc;
+        g.batch.start[k] = total;
+        total += (int)m.dst.size();
+        if (m.needs_scratch) g.two_pass = true;
+    }
+    g.batch.start[maps.size()] = total;
+    g.batch.total = total;
+    if (g.two_pass) h->scratch_doubles = std::max(h->scratch_doubles, (size_t)total * g.ncomp_max);
+    return SALEC_OK;
+}
+
+int run_gather(salec_gpu *h, const Gather &g)
+{
+    if (g.batch.total == 0) return SALEC_OK;
+    const int tb = 256, nb = (g.batch.total + tb - 1) / tb;
+    if (!g.two_pass) {
+        k_gather<<<nb, tb, 0, h->stream>>>(g.batch, 0, nullptr);
+    } else {
+        k_gather<<<nb, tb, 0, h->stream>>>(g.batch, 1, h->scratch);
+        k_gather<<<nb, tb, 0, h->stream>>>(g.batch, 2, h->scratch);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return SALEC_OK;
+}
+
+dim3 grid2(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y); }
+
+int run_phase(salec_gpu *h, int ph)
+{
+    const Ctx c = h->ctx();
+    const dim3 blk(32, 8);
+    const dim3 gc = grid2(h->d.enx, h->d.eny, blk), gv = grid2(h->d.vnx, h->d.vny, blk);
+    cudaStream_t s = h->stream;
+    int rc = SALEC_OK;
+    switch (ph) {
+    case 0: {
+        const int nb = (h->d.enx + 255) / 256;
+        k_profile_reset<<<nb, 256, 0, s>>>(c);
+        k_trace_profile<<<dim3((h->d.enx + 31) / 32, (h->d.eny + 63) / 64), blk, 0, s>>>(c);
+        k_profile_decode<<<nb, 256, 0, s>>>(c);
+        break;
+    }
+    case 1:
+        rc = run_gather(h, h->g_mvof);
+        k_vertex_vof<<<gv, blk, 0, s>>>(c);
+        break;
+    case 2:
+        rc = run_gather(h, h->g_dvel_den);
+        k_vertex_momentum<<<gv, blk, 0, s>>>(c);
+        if (!rc) rc = run_gather(h, h->r_vel);
+        break;
+    case 3:
+        k_cell_velocity<<<gc, blk, 0, s>>>(c);
+        rc = run_gather(h, h->g_evel);
+        break;
+    case 4: k_void_vertices<<<gv, blk, 0, s>>>(c); break;
+    case 5: k_gradient_viscosity_cfl<<<gc, blk, 0, s>>>(c); break;
+    case 6: k_finalize_dt<<<1, 32, 0, s>>>(c); break;
+    case 7: k_stress<<<gc, blk, 0, s>>>(c); break;
+    case 8:
+        rc = run_gather(h, h->g_pre_ste_q);
+        k_vertex_acceleration<<<gv, blk, 0, s>>>(c);
+        if (!rc) rc = run_gather(h, h->r_acc);
+        break;
+    case 9:
+        k_vertex_displacement<<<gv, blk, 0, s>>>(c);
+        rc = run_gather(h, h->r_dis);
+        break;
+    case 10: k_energy<<<gc, blk, 0, s>>>(c); break;
+    case 11: break;   // tracers: see salec_tracer.cu
+    case 12:
+        k_flux<<<gc, blk, 0, s>>>(c, 0);
+        rc = run_gather(h, h->g_flux_state);
+        k_flux<<<gc, blk, 0, s>>>(c, 1);
+        break;
+    case 13: break;   // strength condition from tracers (lubrication is rejected at create)
+    case 14: {
+        const int ejecta = (h->rp.flow_resistance > 0. || h->rp.flow_friction > 0.) ? 1 : 0;
+        k_remap_damp_state<<<gc, blk, 0, s>>>(c, 1, 1, ejecta, 1);
+        break;
+    }
+    case 15: k_cycle<<<1, 32, 0, s>>>(c); break;
+    default: return fail(SALEC_ERR_ARG, "phase out of range");
+    }
+    if (rc) return rc;
+    CUDA_TRY(cudaGetLastError());
+    return SALEC_OK;
+}
+
+int build_gathers(salec_gpu *h)
+{
+    const Dims &d = h->d;
+    auto gm = [&](const char *name, GhostPattern pat) {
+        int fid = field_by_name(name);
+        return std::make_pair(fid, build_ghost_map(d.enx, d.eny, d.P, field_ncomp(h, fid), h->go, pat));
+    };
+    auto rm = [&](const char *name) {
+        int fid = field_by_name(name);
+        return std::make_pair(fid, build_restrict_map(d.vnx, d.vny, d.P, field_ncomp(h, fid), h->go));
+    };
+    int rc;
+    if ((rc = make_gather(h, h->g_mvof, {gm("m_vof", GP_ALWAYS_COPY)}))) return rc;
+    if ((rc = make_gather(h, h->g_dvel_den, {gm("e_dvel", GP_VELOCITY_INC), gm("e_den", GP_DENSITY)}))) return rc;
+    if ((rc = make_gather(h, h->g_evel, {gm("e_vel", GP_VELOCITY)}))) return rc;
+    if ((rc = make_gather(h, h->g_pre_ste_q,
+                          {gm("e_pre", GP_ALWAYS_COPY), gm("e_ste", GP_STRESS), gm("e_q", GP_ALWAYS_COPY)})))
+        return rc;
+    std::vector<std::pair<int, GatherMap>> fs = {gm("m_den", GP_DENSITY), gm("e_vib", GP_ALWAYS_COPY),
+                                                 gm("m_eng", GP_DENSITY)};
+    if (h->rp.porosity_model) {
+        fs.push_back(gm("m_pty", GP_ALWAYS_COPY));
+        fs.push_back(gm("e_cvs", GP_ALWAYS_COPY));
+    }
+    if ((rc = make_gather(h, h->g_flux_state, fs))) return rc;
+    if ((rc = make_gather(h, h->r_vel, {rm("v_vel")}))) return rc;
+    if ((rc = make_gather(h, h->r_acc, {rm("v_acc")}))) return rc;
+    if ((rc = make_gather(h, h->r_dis, {rm("v_dis")}))) return rc;
+    if (h->scratch_doubles) {
+        void *p = nullptr;
+        CUDA_TRY(cudaMalloc(&p, h->scratch_doubles * sizeof(double)));
+        h->owned.push_back(p);
+        h->scratch = static_cast<double *>(p);
+    }
+    return SALEC_OK;
+}
+
+int upload_material(salec_gpu *h, const salec_material_desc &m, DevMat &dm)
+{
+    memset(&dm, 0, sizeof(dm));
+    dm.eos_type = m.eos_type;
+    dm.yfunc = m.yfunc; dm.tfunc = m.tfunc; dm.dsdf = m.dsdf; dm.porfunc = m.porfunc;
+    dm.PolyLiq = m.PolyLiq; dm.PolySol = m.PolySol;
+#define CP(x) dm.x = m.x
+    CP(VaporDen); CP(MeltDen); CP(GaCoef); CP(Yint0); CP(Yfricint); CP(Ylimint); CP(Ydam0); CP(Yfricdam);
+    CP(Ylimdam); CP(Yten0); CP(IvanA); CP(IvanB); CP(IvanC); CP(Pbd); CP(Pbp); CP(minPint); CP(minPdam);
+    CP(JCA); CP(JCB); CP(JCN); CP(JCC); CP(JCM); CP(JCTREF); CP(JCMaxPlastic); CP(Asimon); CP(Csimon);
+    CP(Tmelt0); CP(Tfrac); CP(Tdelta); CP(Tlidc1); CP(Tlidc2); CP(Tlidc3); CP(Tsolc1); CP(Tsolc2);
+    CP(Tsolc3); CP(Toff); CP(Cvib); CP(VibMax); CP(Tdamp); CP(Pvlim); CP(Acvis); CP(alpha0); CP(alphax);
+    CP(epse0); CP(chi); CP(kappa); CP(avel); CP(epsec); CP(epsex); CP(alphamax); CP(alphamax2); CP(alphae);
+    CP(gamfrac); CP(melt_viscosity);
+#undef CP
+    for (int k = 0; k < 13; ++k) dm.tl[k] = m.till[k];
+    int rc;
+    if (m.eos_type == SALEC_EOS_TILLOTSON) {
+        if (m.cold_n < 2 || !m.cold_yeng) return fail(SALEC_ERR_ARG, "Tillotson material without cold-energy curve");
+        dm.cold_n = m.cold_n;
+        std::vector<double> y(m.cold_yeng, m.cold_yeng + m.cold_n);
+        if ((rc = upload_vec(h, y, &dm.cold_yeng))) return rc;
+    } else if (m.eos_type == SALEC_EOS_ANEOS || m.eos_type == SALEC_EOS_ANEOS_SIEDEN) {
+        if (m.ntem < 2 || m.nden < 2 || !m.xtem || !m.yden || !m.data) return fail(SALEC_ERR_ARG, "table EOS without table");
+        dm.ntem = m.ntem;
+        dm.nden = m.nden;
+        std::vector<double> x(m.xtem, m.xtem + m.ntem), y(m.yden, m.yden + m.nden);
+        std::vector<double> t(m.data, m.data + (size_t)m.ntem * m.nden * 3);
+        if ((rc = upload_vec(h, x, &dm.xtem))) return rc;
+        if ((rc = upload_vec(h, y, &dm.yden))) return rc;
+        if ((rc = upload_vec(h, t, &dm.data))) return rc;
+    } else {
+        return fail(SALEC_ERR_ARG, "unknown EOS type");
+    }
+    return SALEC_OK;
+}
+
+int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
+{
+    if (fid < 0 || fid >= kNumFields) return fail(SALEC_ERR_ARG, "unknown field");
+    int nx, ny;
+    field_points(h, fid, nx, ny);
+    const int nc = field_ncomp(h, fid);
+    const long long need = (long long)nx * ny * nc;
+    if (n != need) return fail(SALEC_ERR_ARG, std::string("field ") + kFields[fid].name + ": expected " +
+                                                  std::to_string(need) + " doubles, got " + std::to_string(n));
+    if ((size_t)need > h->staging_doubles) {
+        if (h->staging) cudaFree(h->staging);
+        h->staging = nullptr;
+        CUDA_TRY(cudaMalloc(&h->staging, need * sizeof(double)));
+        h->staging_doubles = need;
+    }
+    double *base = field_ptr(h, fid);
+    const long long plane = kFields[fid].loc == L_COL ? 0 : h->d.PL;
+    const int tb = 256;
+    const int nb = (int)(((long long)nx * ny + tb - 1) / tb);
+    if (to_device) {
+        CUDA_TRY(cudaMemcpyAsync(h->staging, host, need * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        k_aos_to_planes<<<nb, tb, 0, h->stream>>>(h->staging, base, plane, h->d.P, nx, ny, nc);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+    } else {
+        k_planes_to_aos<<<nb, tb, 0, h->stream>>>(base, h->staging, plane, h->d.P, nx, ny, nc);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(host, h->staging, need * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+    return SALEC_OK;
+}
+
+void release(salec_gpu *h)
+{
+    if (!h) return;
+    for (void *p : h->owned) cudaFree(p);
+    if (h->pool) cudaFree(h->pool);
+    if (h->staging) cudaFree(h->staging);
+    if (h->scal) cudaFree(h->scal);
+    if (h->scal_host) cudaFreeHost(h->scal_host);
+    if (h->mat) cudaFree(h->mat);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+} // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+const char *salec_gpu_last_error(void) { return g_last_error.c_str(); }
+
+int salec_gpu_func_index(const char *name)
+{
+    if (!name) return -1;
+    for (int k = 0; k < (int)(sizeof(kFuncNames) / sizeof(kFuncNames[0])); ++k) {
+        const char *a = kFuncNames[k], *b = name;
+        while (*a && *b && tolower((unsigned char)*a) == tolower((unsigned char)*b)) { ++a; ++b; }
+        if (*a == 0 && *b == 0) return k;
+    }
+    return -1;
+}
+
+int salec_gpu_field_index(const char *name) { return field_by_name(name); }
+
+int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats, salec_gpu **out)
+{
+    if (!run || !mats || !out) return fail(SALEC_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (run->nx < 4 || run->ny < 4) return fail(SALEC_ERR_ARG, "mesh must have at least 4x4 cells");
+    if (run->nmat < 2 || run->nmat > SALEC_MAXMAT) return fail(SALEC_ERR_ARG, "nmat must be in [2, 10]");
+    if (run->tracer_lubrication > 0)
+        return fail(SALEC_ERR_UNSUPPORTED, "tracer lubrication (tracer.lubrication > 0) is not supported");
+    if (run->damp_type < 0 || run->damp_type > 5) return fail(SALEC_ERR_ARG, "unknown damping type");
+    if (run->damp_type == SALEC_DAMP_PML3)
+        return fail(SALEC_ERR_UNSUPPORTED, "damping = pml3 (advect_flux_pml3) is not supported yet");
+    salec_gpu *h = new salec_gpu();
+    Dims &d = h->d;
+    d.nmat = run->nmat;
+    d.enx = run->nx + 4;
+    d.eny = run->ny + 4;
+    d.vnx = run->nx + 5;
+    d.vny = run->ny + 5;
+    d.phi = 3 * d.nmat + 10 + (run->porosity_model ? d.nmat + 1 : 0);
+    d.P = ((d.vnx + 31) / 32) * 32;
+    d.R = d.vny;
+    d.PL = (((long long)d.P * d.R + 31) / 32) * 32;
+    for (int k = 0; k < 4; ++k) h->go[k] = run->go[k];
+    RunParams &rp = h->rp;
+    rp.damp_type = run->damp_type; rp.partpres = run->partpres; rp.porosity_model = run->porosity_model;
+    rp.acoustic_fluid = run->acoustic_fluid; rp.tensile_failure = run->tensile_failure;
+    rp.tracer_lubrication = run->tracer_lubrication;
+    rp.avis1 = run->avis1; rp.avis2 = run->avis2; rp.anc = run->anc;
+    rp.density_cutoff = run->density_cutoff; rp.velocity_max = run->velocity_max;
+    rp.velocity_min = run->velocity_min; rp.acceleration_min = run->acceleration_min;
+    rp.alpha_damp_x = run->alpha_damp_x; rp.alpha_damp_y = run->alpha_damp_y; rp.damp_time = run->damp_time;
+    rp.threshold_z = run->threshold_z; rp.flow_resistance = run->flow_resistance;
+    rp.flow_friction = run->flow_friction; rp.tracer_lub_y0 = run->tracer_lub_y0;
+    rp.tracer_lub_frac = run->tracer_lub_frac; rp.max_dt = run->max_dt;
+
+    auto bail = [&](int rc) { release(h); return rc; };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(SALEC_ERR_CUDA, "cudaStreamCreate failed"));
+
+    // one pool, every component plane 256-byte aligned
+    size_t planes = 0;
+    for (int k = 0; k < kNumFields; ++k) planes += kFields[k].loc == L_COL ? 0 : (size_t)field_ncomp(h, k);
+    const size_t col = (((size_t)d.enx + 31) / 32) * 32;
+    h->pool_doubles = planes * (size_t)d.PL + col;
+    if (cudaMalloc(&h->pool, h->pool_doubles * sizeof(double)) != cudaSuccess)
+        return bail(fail(SALEC_ERR_ALLOC, "device pool of " + std::to_string(h->pool_doubles * 8) + " bytes"));
+    if (cudaMemsetAsync(h->pool, 0, h->pool_doubles * sizeof(double), h->stream) != cudaSuccess)
+        return bail(fail(SALEC_ERR_CUDA, "pool memset failed"));
+    size_t off = 0;
+    for (int k = 0; k < kNumFields; ++k) {
+        field_ptr(h, k) = h->pool + off;
+        off += kFields[k].loc == L_COL ? col : (size_t)field_ncomp(h, k) * d.PL;
+    }
+
+    std::vector<DevMat> dms(d.nmat);
+    memset(dms.data(), 0, sizeof(DevMat) * d.nmat);
+    for (int m = 1; m < d.nmat; ++m) {
+        int rc = upload_material(h, mats[m], dms[m]);
+        if (rc) return bail(rc);
+    }
+    if (cudaMalloc(&h->mat, sizeof(DevMat) * d.nmat) != cudaSuccess) return bail(fail(SALEC_ERR_ALLOC, "materials"));
+    if (cudaMemcpy(h->mat, dms.data(), sizeof(DevMat) * d.nmat, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(SALEC_ERR_CUDA, "material upload"));
+
+    if (cudaMalloc(&h->scal, sizeof(Scal)) != cudaSuccess) return bail(fail(SALEC_ERR_ALLOC, "scalars"));
+    if (cudaMallocHost(&h->scal_host, sizeof(Scal)) != cudaSuccess) return bail(fail(SALEC_ERR_ALLOC, "scalars"));
+    Scal s0{};
+    s0.dt = run->dt;
+    s0.time = run->time;
+    s0.i_step = run->i_step;
+    s0.dt_acc = ord_encode(1.1 * run->dt);
+    if (cudaMemcpy(h->scal, &s0, sizeof(Scal), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(SALEC_ERR_CUDA, "scalar upload"));
+
+    int rc = build_gathers(h);
+    if (rc) return bail(rc);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(SALEC_ERR_CUDA, "create sync"));
+    *out = h;
+    return SALEC_OK;
+}
+
+int salec_gpu_destroy(salec_gpu *h)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    cudaStreamSynchronize(h->stream);
+    release(h);
+    return SALEC_OK;
+}
+
+int salec_gpu_field_shape(const salec_gpu *h, int field, int *nx, int *ny, int *ncomp)
+{
+    if (!h || field < 0 || field >= kNumFields) return fail(SALEC_ERR_ARG, "bad handle or field");
+    int a, b;
+    field_points(h, field, a, b);
+    if (nx) *nx = a;
+    if (ny) *ny = b;
+    if (ncomp) *ncomp = field_ncomp(h, field);
+    return SALEC_OK;
+}
+
+int salec_gpu_set_field(salec_gpu *h, int field, const double *host, long long n)
+{
+    if (!h || !host) return fail(SALEC_ERR_ARG, "null argument");
+    return transfer(h, field, const_cast<double *>(host), n, true);
+}
+
+int salec_gpu_get_field(salec_gpu *h, int field, double *host, long long n)
+{
+    if (!h || !host) return fail(SALEC_ERR_ARG, "null argument");
+    return transfer(h, field, host, n, false);
+}
+
+int salec_gpu_phases(salec_gpu *h, int first, int last)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    if (first < 0 || last > 15 || first > last) return fail(SALEC_ERR_ARG, "phase range must lie in [0, 15]");
+    for (int p = first; p <= last; ++p) {
+        int rc = run_phase(h, p);
+        if (rc) return rc;
+    }
+    return SALEC_OK;
+}
+
+int salec_gpu_step(salec_gpu *h, int nsteps)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    if (nsteps < 0) return fail(SALEC_ERR_ARG, "negative step count");
+    for (int k = 0; k < nsteps; ++k) {
+        int rc = salec_gpu_phases(h, 0, 15);
+        if (rc) return rc;
+    }
+    return SALEC_OK;
+}
+
+int salec_gpu_sync(salec_gpu *h)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return SALEC_OK;
+}
+
+int salec_gpu_get_scalar(salec_gpu *h, const char *name, double *value)
+{
+    if (!h || !name || !value) return fail(SALEC_ERR_ARG, "null argument");
+    CUDA_TRY(cudaMemcpyAsync(h->scal_host, h->scal, sizeof(Scal), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const Scal &s = *h->scal_host;
+    if (!strcmp(name, "dt")) *value = s.dt;
+    else if (!strcmp(name, "time")) *value = s.time;
+    else if (!strcmp(name, "i_step")) *value = (double)s.i_step;
+    else if (!strcmp(name, "dt_candidate")) *value = ord_decode(s.dt_acc);
+    else if (!strcmp(name, "damp_time")) *value = h->rp.damp_time;
+    else if (!strcmp(name, "max_dt")) *value = h->rp.max_dt;
+    else return fail(SALEC_ERR_ARG, std::string("unknown scalar ") + name);
+    return SALEC_OK;
+}
+
+int salec_gpu_set_scalar(salec_gpu *h, const char *name, double value)
+{
+    if (!h || !name) return fail(SALEC_ERR_ARG, "null argument");
+    if (!strcmp(name, "damp_time")) { h->rp.damp_time = value; return SALEC_OK; }
+    if (!strcmp(name, "max_dt")) { h->rp.max_dt = value; return SALEC_OK; }
+    CUDA_TRY(cudaMemcpyAsync(h->scal_host, h->scal, sizeof(Scal), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    Scal s = *h->scal_host;
+    if (!strcmp(name, "dt")) { s.dt = value; s.dt_acc = ord_encode(1.1 * value); }
+    else if (!strcmp(name, "time")) s.time = value;
+    else if (!strcmp(name, "i_step")) s.i_step = (long long)value;
+    else return fail(SALEC_ERR_ARG, std::string("unknown scalar ") + name);
+    *h->scal_host = s;
+    CUDA_TRY(cudaMemcpyAsync(h->scal, h->scal_host, sizeof(Scal), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return SALEC_OK;
+}
+
+int salec_gpu_set_tracers(salec_gpu *h, int n, const double *rows)
+{
+    (void)rows;
+    if (!h || n < 0) return fail(SALEC_ERR_ARG, "bad argument");
+    h->ntracer = n;
+    return SALEC_OK;
+}
+
+int salec_gpu_get_tracers(salec_gpu *h, double *rows, int *n)
+{
+    (void)rows;
+    if (!h || !n) return fail(SALEC_ERR_ARG, "bad argument");
+    *n = 0;
+    return SALEC_OK;
+}
+
+int salec_gpu_check(salec_gpu *h, long long *n_bad)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    unsigned long long *cnt = &h->scal->nan_count;
+    CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), h->stream));
+    const char *names[] = {"v_vel", "v_acc", "v_dis", "e_vel", "e_ste", "e_dvel", "e_pre", "e_den", "e_csd",
+                           "m_vof", "m_den", "m_eng"};
+    for (const char *nm : names) {
+        int fid = field_by_name(nm);
+        const long long n = (long long)field_ncomp(h, fid) * h->d.PL;
+        k_count_nonfinite<<<592, 256, 0, h->stream>>>(field_ptr(h, fid), n, cnt);
+    }
+    CUDA_TRY(cudaGetLastError());
+    unsigned long long bad = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h->scal_host->nan_count, cnt, sizeof(bad), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    bad = h->scal_host->nan_count;
+    if (n_bad) *n_bad = (long long)bad;
+    return bad ? fail(SALEC_ERR_NUMERIC, std::to_string(bad) + " non-finite values") : SALEC_OK;
+}
+
+} // extern "C"

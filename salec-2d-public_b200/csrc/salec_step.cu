@@ -1,0 +1,1304 @@
+// Step kernels of the B200 mesh update (FP64 form).
+//
+// One kernel per sweep group of the reference's time loop (src/salec2d.c:115-272); each
+// thread owns one cell or one vertex, which is exactly the reference's Jacobi structure:
+// every sweep writes only its own point (or, in the flux sweep, only the faces on which its
+// own cell is the upwind donor). Cross-point boundary fills (ghost cells and restricted
+// vertices) are separate gather passes, see salec_ghost.cpp.
+//
+// Point sections (src/mpi_vec/mpi_vec.c:111-230, one rank):
+//   cells:    interior = 2 <= i <= enx-3 and 2 <= j <= eny-3 (internal|send); the rest is pad.
+//   vertices: active = 1 <= i <= vnx-2 and 1 <= j <= vny-2 (update|internal); the outer ring is
+//             never updated; "pad_section" = x or y distance to the outer ring <= 1.
+#include "salec_device.cuh"
+#include "salec_kernels.h"
+
+namespace salec {
+
+#define KIDX(i, j) ((long long)(i) + (long long)c.d.P * (long long)(j))
+#define PLN(ptr, comp) ((ptr) + (long long)(comp) * c.d.PL)
+
+__device__ __forceinline__ bool cell_interior(const Ctx &c, int i, int j)
+{
+    return i >= 2 && i <= c.d.enx - 3 && j >= 2 && j <= c.d.eny - 3;
+}
+__device__ __forceinline__ bool vert_active(const Ctx &c, int i, int j)
+{
+    return i >= 1 && i <= c.d.vnx - 2 && j >= 1 && j <= c.d.vny - 2;
+}
+__device__ __forceinline__ bool vert_pad(const Ctx &c, int i, int j)
+{
+    int xd = min(i, c.d.vnx - 1 - i), yd = min(j, c.d.vny - 1 - j);
+    return xd <= 1 || yd <= 1;
+}
+__device__ __forceinline__ double step_dt(const Ctx &c)
+{
+    // Min(max_dt, CFL reduction) as in src/salec2d.c:167
+    double r = ord_decode(c.scal->dt_acc);
+    return dmin(c.rp.max_dt, r);
+}
+
+// ============================================================ phase 0: surface profile
+// trace_profile (src/ejecta.c:8-63): per column, MIN of cell-centre y over cells whose vacuum
+// fraction exceeds 0.1; cells above the ejecta threshold with no vacuum get e_ejt = 1.
+__global__ void k_profile_reset(const Ctx c)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < c.d.enx) c.f.y_profile[i] = __longlong_as_double((long long)ord_encode(c.rp.threshold_z * 2.0));
+}
+
+__global__ void k_trace_profile(const Ctx c)
+{
+    __shared__ unsigned long long smin[8][32];
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j0 = blockIdx.y * 64 + threadIdx.y;
+    unsigned long long best = ~0ULL;
+    if (i < c.d.enx) {
+        for (int j = j0; j < min(c.d.eny, (int)blockIdx.y * 64 + 64); j += 8) {
+            long long p = KIDX(i, j);
+            double v0 = c.f.m_vof[p];
+            double y = PLN(c.f.e_pos, 1)[p];
+            if (v0 > 0.1) best = min(best, ord_encode(y));
+            if (y > c.rp.threshold_z && v0 < SALEC_TOLVOF) c.f.e_ejt[p] = 1.0;
+        }
+    }
+    smin[threadIdx.y][threadIdx.x] = best;
+    __syncthreads();
+    if (threadIdx.y == 0 && i < c.d.enx) {
+        for (int k = 1; k < 8; ++k) best = min(best, smin[k][threadIdx.x]);
+        if (best != ~0ULL) atomicMin((unsigned long long *)&c.f.y_profile[i], best);
+    }
+}
+
+__global__ void k_profile_decode(const Ctx c)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < c.d.enx) {
+        unsigned long long u = (unsigned long long)__double_as_longlong(c.f.y_profile[i]);
+        c.f.y_profile[i] = ord_decode(u);
+    }
+}
+
+// ============================================================ phase 1: vertex volume fractions
+// update_v_vof (src/sale2d.c:751-791): mean of the four surrounding cells.
+__global__ void k_vertex_vof(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!vert_active(c, i, j)) return;
+    const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
+    const long long p = KIDX(i, j);
+    for (int m = 0; m < c.d.nmat; ++m) {
+        const double *ev = PLN(c.f.m_vof, m);
+        double s = 0.0;
+        for (int k = 0; k < 4; ++k) s += 0.25 * ev[cl[k]];
+        PLN(c.f.v_vof, m)[p] = s;
+    }
+}
+
+// ============================================================ phase 2: vertex momentum
+// update_v_vel_inc (src/sale2d.c:930-1049): add the advected momentum increments of the
+// four cells, weighted by density and corner sub-volume; clamp |v|; count void corners.
+__global__ void k_vertex_momentum(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!vert_active(c, i, j)) return;
+    const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
+    const int corner[4] = {2, 3, 0, 1};
+    const long long p = KIDX(i, j);
+    double *vx = c.f.v_vel, *vy = PLN(c.f.v_vel, 1);
+    double *m0 = c.f.v_mass, *m1 = PLN(c.f.v_mass, 1);
+    const double old_x = vx[p], old_y = vy[p];
+    double inc_x = 0., inc_y = 0., vvol = 0., vmass = 0.;
+    int void_corner = 0;
+    for (int k = 0; k < 4; ++k) {
+        if (PLN(c.f.e_wpt, corner[k])[cl[k]] > 0.) void_corner++;
+        const double rho = c.f.e_den[cl[k]];
+        if (rho < SALEC_TOLRHO) continue;
+        const double lv = PLN(c.f.v_vol, k + 1)[p];
+        vvol += lv;
+        vmass += rho * lv;
+        const double w = rho * lv;
+        inc_x += w * c.f.e_dvel[cl[k]];
+        inc_y += w * PLN(c.f.e_dvel, 1)[cl[k]];
+    }
+    double nx_, ny_;
+    if (vmass > SALEC_TOLRHO * vvol) {
+        const double pa = 1.0 / vmass, pb = m0[p] / vmass;
+        nx_ = pa * inc_x + pb * old_x;
+        ny_ = pa * inc_y + pb * old_y;
+        m0[p] = vmass;
+    } else {
+        m0[p] = 0.;
+        nx_ = 0.; ny_ = 0.;
+    }
+    m1[p] = 1.0 * void_corner;
+    double vn = 0.;
+    vn += nx_ * nx_;
+    vn += ny_ * ny_;
+    vn = sqrt(vn);
+    if (vn > c.rp.velocity_max) {
+        const double s = c.rp.velocity_max / vn;
+        nx_ *= s; ny_ *= s;
+    }
+    if (vn < c.rp.velocity_min * 1) { nx_ = 0.; ny_ = 0.; }
+    vx[p] = nx_; vy[p] = ny_;
+}
+
+// ============================================================ phase 3: cell velocity
+// update_e_vel (src/sale2d.c:838-928): mass-weighted mean over the solid corner vertices.
+__global__ void k_cell_velocity(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!cell_interior(c, i, j)) return;
+    const long long p = KIDX(i, j);
+    const long long vl[4] = {KIDX(i, j), KIDX(i + 1, j), KIDX(i + 1, j + 1), KIDX(i, j + 1)};
+    double ex = 0., ey = 0.;
+    const double rho = c.f.e_den[p];
+    if (!(rho < SALEC_TOLRHO)) {
+        int vac = 0;
+        double wpt[4];
+        for (int k = 0; k < 4; ++k) {
+            wpt[k] = PLN(c.f.e_wpt, k)[p];
+            const double nvoid = PLN(c.f.v_mass, 1)[vl[k]];
+            if (nvoid >= 4.0 || (nvoid >= 3.0 && wpt[k] < 0.)) vac++;
+        }
+        if (vac != 4) {
+            double sm = 0.;
+            for (int k = 0; k < 4; ++k) {
+                if (wpt[k] > 0.0 || rho < SALEC_TOLRHO) continue;
+                const double mk = c.f.v_mass[vl[k]];
+                ex += mk * c.f.v_vel[vl[k]];
+                ey += mk * PLN(c.f.v_vel, 1)[vl[k]];
+                sm += mk;
+            }
+            if (sm > 0.) {
+                const double s = 1.0 / sm;
+                ex *= s; ey *= s;
+            } else {
+                ex = 0.; ey = 0.;
+            }
+        }
+    }
+    c.f.e_vel[p] = ex;
+    PLN(c.f.e_vel, 1)[p] = ey;
+}
+
+// ============================================================ phase 4: void vertices
+// check_v_vel (src/sale2d.c:1051-1142): a vertex whose four corners are all void takes the
+// density-weighted velocity of its non-empty cells.
+__global__ void k_void_vertices(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!vert_active(c, i, j)) return;
+    const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
+    const int corner[4] = {2, 3, 0, 1};
+    int void_cell = 0, void_corner = 0;
+    for (int k = 0; k < 4; ++k) {
+        if (c.f.e_den[cl[k]] < SALEC_TOLRHO) void_cell++;
+        if (PLN(c.f.e_wpt, corner[k])[cl[k]] > 0.) void_corner++;
+    }
+    if (void_cell >= 4 || void_corner < 4) return;
+    double ax = 0., ay = 0., ad = 0.;
+    for (int k = 0; k < 4; ++k) {
+        const double rho = c.f.e_den[cl[k]];
+        if (rho < SALEC_TOLRHO) continue;
+        ad += rho;
+        ax += rho * c.f.e_vel[cl[k]];
+        ay += rho * PLN(c.f.e_vel, 1)[cl[k]];
+    }
+    const double s = 1.0 / ad;
+    const long long p = KIDX(i, j);
+    c.f.v_vel[p] = s * ax;
+    PLN(c.f.v_vel, 1)[p] = s * ay;
+}
+
+// ============================================================ phase 5 (+6): velocity gradient,
+// artificial viscosity and the CFL candidate of every interior cell.
+// update_e_gradvel (src/sale2d.c:1144-1236) and calculate_dt (src/sale2d.c:1959-2016).
+__global__ void k_gradient_viscosity_cfl(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    unsigned long long cand = ~0ULL;
+    if (cell_interior(c, i, j)) {
+        const long long p = KIDX(i, j);
+        const long long vl[4] = {KIDX(i, j), KIDX(i + 1, j), KIDX(i + 1, j + 1), KIDX(i, j + 1)};
+        double vx[4], vy[4];
+        for (int k = 0; k < 4; ++k) { vx[k] = c.f.v_vel[vl[k]]; vy[k] = PLN(c.f.v_vel, 1)[vl[k]]; }
+        double g[12];
+        for (int k = 0; k < 12; ++k) g[k] = PLN(c.f.e_grad, k)[p];
+        double d0 = 0., d1 = 0., d2 = 0., d3 = 0., d4 = 0.;
+        for (int k = 0; k < 4; ++k) d0 += g[k] * vx[k];        // dv_r/dr
+        for (int k = 0; k < 4; ++k) d2 += g[k] * vy[k];        // dv_z/dr
+        for (int k = 0; k < 4; ++k) d1 += g[4 + k] * vx[k];    // dv_r/dz
+        for (int k = 0; k < 4; ++k) d3 += g[4 + k] * vy[k];    // dv_z/dz
+        for (int k = 0; k < 4; ++k) d4 += g[8 + k] * vx[k];    // v_r/r
+        PLN(c.f.e_grad_vel, 0)[p] = d0;
+        PLN(c.f.e_grad_vel, 1)[p] = d1;
+        PLN(c.f.e_grad_vel, 2)[p] = d2;
+        PLN(c.f.e_grad_vel, 3)[p] = d3;
+        PLN(c.f.e_grad_vel, 4)[p] = d4;
+        const double div = d0 + d3 + d4;
+        c.f.e_div_vel[p] = div;
+        const double vof0 = c.f.m_vof[p];
+        const double csd = c.f.e_csd[p];
+        double q;
+        if (vof0 > SALEC_TOLVOF || c.f.e_pre[p] <= 0.0) {
+            q = 0.;
+        } else {
+            double area = c.f.e_vol[p] / c.f.e_pos[p];
+            area = fabs(area);
+            const double ql = c.rp.avis1 * csd * sqrt(area);
+            const double qq = c.rp.avis2 * div * area;
+            q = dmin(0., div) * c.f.e_den[p] * (qq - ql);
+            if (q < SALEC_TOLQPRE) q = 0.;
+        }
+        c.f.e_q[p] = q;
+        // CFL candidate over cells that are not pure vacuum
+        if (!(vof0 > 1.0 - SALEC_TOLVOF)) {
+            const double dt_r = 1.0 * PLN(c.f.e_pos, 2)[p] / (fabs(c.f.e_vel[p]) + csd);
+            const double dt_z = 1.0 * PLN(c.f.e_pos, 3)[p] / (fabs(PLN(c.f.e_vel, 1)[p]) + csd);
+            const double dt_rz = SALEC_DTF * dmin(dt_r, dt_z);
+            cand = ord_encode(dt_rz);
+        }
+    }
+    // block MIN, one atomic per block
+    for (int o = 16; o > 0; o >>= 1) cand = min(cand, __shfl_xor_sync(0xffffffffu, cand, o));
+    __shared__ unsigned long long wmin[32];
+    const int lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31;
+    const int warp = (threadIdx.y * blockDim.x + threadIdx.x) >> 5;
+    if (lane == 0) wmin[warp] = cand;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+        unsigned long long v = lane < nw ? wmin[lane] : ~0ULL;
+        for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0 && v != ~0ULL) atomicMin(&c.scal->dt_acc, v);
+    }
+}
+
+// phase 6: dt of this cycle (single thread)
+__global__ void k_finalize_dt(const Ctx c)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) c.scal->dt = step_dt(c);
+}
+
+// ============================================================ phase 7: vibration, stress, damage
+// block_vibration (src/strength.c:625-695) and update_e_stress (src/strength.c:7-349).
+__global__ void k_stress(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!cell_interior(c, i, j)) return;
+    const long long p = KIDX(i, j);
+    const int nmat = c.d.nmat;
+    const double dt = c.scal->dt;
+    const double vof0 = c.f.m_vof[p];
+    double dam = c.f.e_dam[p];
+
+    // --- acoustic fluidisation (block model)
+    if (c.rp.acoustic_fluid) {
+        double vib = c.f.e_vib[p];
+        if (vof0 > SALEC_TOLVOF || dam < 0.5) {
+            vib = 0.;
+        } else {
+            double tdec = -1.0, cvib = 0.0, toff = -1.0, vmax = 0.0, pvl = 0.0;
+            for (int m = 1; m < nmat; ++m) {
+                if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
+                const DevMat &s = c.mat[m];
+                tdec = dmax(s.Tdamp, tdec);
+                cvib = dmax(s.Cvib, cvib);
+                toff = dmax(s.Toff, toff);
+                vmax = dmax(s.VibMax, vmax);
+                pvl = dmax(s.Pvlim, pvl);
+            }
+            if (tdec <= 0. || toff <= 0.) {
+                vib = 0.;
+            } else {
+                const double evx = c.f.e_vel[p], evy = PLN(c.f.e_vel, 1)[p];
+                double len = 0.;
+                len += evx * evx;
+                len += evy * evy;
+                const double nv = cvib * sqrt(len);
+                const double nv2 = nv * nv;
+                const double t = c.scal->time;
+                if ((t <= toff) && (nv2 >= vib) && (nv >= 1.0) && (c.f.e_q[p] > 0.))
+                    vib = dmin(nv2, vmax * vmax);
+                else
+                    vib = dmax(vib * (1.0 - 2.0 * dt / tdec + 2.0 * (dt / tdec) * (dt / tdec)), 0.0);
+            }
+        }
+        c.f.e_vib[p] = vib;
+    }
+
+    // --- stress update
+    double s0 = c.f.e_ste[p], s1 = PLN(c.f.e_ste, 1)[p], s2 = PLN(c.f.e_ste, 2)[p], s3 = PLN(c.f.e_ste, 3)[p];
+    double ste2s = c.f.e_ste2s[p], sta2s = c.f.e_sta2s[p], tps = c.f.e_tps[p], strength = c.f.e_strength[p];
+    if (vof0 > SALEC_TOLVOF) {
+        c.f.e_ste[p] = 0.; PLN(c.f.e_ste, 1)[p] = 0.; PLN(c.f.e_ste, 2)[p] = 0.; PLN(c.f.e_ste, 3)[p] = 0.;
+        c.f.e_ste2s[p] = 0.; c.f.e_sta2s[p] = 0.; c.f.e_strength[p] = 0.;
+        return;
+    }
+    double vapor_ref = 0., melt_ref = 0.;
+    for (int m = 1; m < nmat; ++m) {
+        const double vm = PLN(c.f.m_vof, m)[p];
+        if (vm < SALEC_TOLVOF) continue;
+        vapor_ref += vm * c.mat[m].VaporDen;
+        melt_ref += vm * c.mat[m].MeltDen;
+    }
+    double porosity = 0.0;
+    if (c.rp.porosity_model) {
+        double mv = 0.0;
+        for (int m = 1; m < nmat; ++m) {
+            const double vm = PLN(c.f.m_vof, m)[p];
+            if (vm < SALEC_TOLVOF) continue;
+            porosity += vm * PLN(c.f.m_pty, m)[p];
+            mv += vm;
+        }
+        porosity /= mv;
+    } else {
+        porosity = 1.0;
+    }
+    porosity = dmax(porosity, 1.0);
+    vapor_ref /= porosity;
+    melt_ref /= porosity;
+
+    const double rho = c.f.e_den[p];
+    const double ste2s_old = ste2s;
+    int state; // 0 solid, 1 melt, 2 vapour
+    const double g0 = c.f.e_grad_vel[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
+                 g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
+    if (rho <= vapor_ref) {
+        state = 2;
+        s0 = s1 = s2 = s3 = 0.;
+        ste2s = 0.;
+        tps = 0.;
+        dam = 0.;
+        strength = 0.;
+    } else {
+        double e0 = g0, e1 = 0.5 * g1 + 0.5 * g2, e2 = g3, e3 = g4;
+        const double tr = e0 + e2 + e3;
+        e0 -= tr / 3.0;
+        e2 -= tr / 3.0;
+        e3 -= tr / 3.0;
+        if (rho <= melt_ref) {
+            state = 1;
+            s0 = s1 = s2 = s3 = 0.;
+            ste2s = 0.;
+            sta2s = sqrt(second_inv(e0, e1, e2, e3));
+            tps = dmin(tps + sta2s * dt, 10.);
+            dam = 1.;
+            strength = 0.;
+        } else {
+            state = 0;
+            // Wilkins rotation
+            double sin2o = (g2 - g1) * dt;
+            sin2o = wind(sin2o, -1., 1.);
+            const double cos2o1 = sqrt(1.0 - sin2o * sin2o) - 1.0;
+            const double ss2 = (s0 - s2) / 2.0;
+            const double r0 = ss2 * cos2o1 + s1 * sin2o;
+            const double r1 = s1 * cos2o1 - ss2 * sin2o;
+            const double r2 = -ss2 * cos2o1 - s1 * sin2o;
+            s0 += 1.0 * r0; s1 += 1.0 * r1; s2 += 1.0 * r2; s3 += 1.0 * 0.0;
+            const double k2 = 2.0 * c.f.e_mu[p] * dt;
+            s0 += k2 * e0; s1 += k2 * e1; s2 += k2 * e2; s3 += k2 * e3;
+            ste2s = sqrt(second_inv(s0, s1, s2, s3));
+            sta2s = sqrt(second_inv(e0, e1, e2, e3));
+        }
+    }
+
+    if (state == 2) {
+        dam = 0.;
+    } else if (state == 1) {
+        dam = 1.0;
+    } else {
+        const double pre = c.f.e_pre[p], tem = c.f.e_tem[p];
+        double shear = 0.0, tensile = 0.;
+        for (int m = 1; m < nmat; ++m) {
+            const double vm = PLN(c.f.m_vof, m)[p];
+            if (vm < SALEC_TOLVOF) continue;
+            const DevMat &s = c.mat[m];
+            double pa[6] = {pre, dam, tps, sta2s, tem, 0.};
+            double my = strength_fn(s.yfunc, pa, s);
+            if (c.rp.acoustic_fluid && pre >= 0.) {
+                const double vibp = dmin(rho * c.f.e_csd[p] * sqrt(c.f.e_vib[p]), pre);
+                const double tm = simon_melt(pre, s);
+                double soft = ohnaka_soft(tem, s, tm);
+                soft = wind(soft, 0.0, 1.0);
+                const double lp = pre - vibp * dam * dam * sqrt(soft);
+                double pb[6] = {lp, dam, tps, sta2s, tem, 0.};
+                const double myv = strength_fn(s.yfunc, pb, s) + rho * s.Acvis * sta2s;
+                my = dmin(myv, my);
+            }
+            shear += vm * dmax(my, 0.0);
+            if (c.rp.tensile_failure) tensile += vm * strength_fn(s.tfunc, pa, s);
+        }
+        if (c.rp.tracer_lubrication >= 1 && c.f.e_cnd[p] >= 1.0) {
+            const double lub = dmin(pre * c.rp.tracer_lub_frac + c.rp.tracer_lub_y0, 0.0);
+            shear = dmin(shear, lub);
+        }
+        strength = shear;
+        if (shear < ste2s) {
+            sta2s = sta2s / dmax(0.5, (ste2s - ste2s_old) / (ste2s - shear));
+            const double sfac = shear / ste2s;
+            s0 *= sfac; s1 *= sfac; s2 *= sfac; s3 *= sfac;
+            ste2s = shear;
+            double dsd = 0.;
+            for (int m = 1; m < nmat; ++m) {
+                const DevMat &s = c.mat[m];
+                double pa[6] = {pre, dam, 0., 0., 0., 0.};
+                dsd += PLN(c.f.m_vof, m)[p] * strength_fn(s.dsdf, pa, s);
+            }
+            dam = wind(dam + sta2s * dsd * dt, 0.0, 1.0);
+            tps = dmin(tps + sta2s * dt, 10.);
+        }
+        if (c.rp.tensile_failure) {
+            const double sxx = s0, szz = s2, sxz = s1, sth = s3;
+            const double ts = sqrt(sxz * sxz + 0.25 * (sxx - szz) * (sxx - szz));
+            double tmax = dmax(0.5 * (sxx + szz) - ts, 0.5 * (sxx + szz) + ts);
+            tmax = dmax(tmax, sth);
+            if ((tmax - pre) > tensile) {
+                // the reference divides by Min(e_pos[1], e_pos[2]) (centre y and scale x)
+                const double dinc = 0.4 * c.f.e_csd[p] / dmin(PLN(c.f.e_pos, 1)[p], PLN(c.f.e_pos, 2)[p]);
+                const double dold = dam;
+                double third = pow(dold, 1.0 / 3.);
+                third += dinc;
+                dam = wind(pow(third, 3.0), 0., 1.);
+                const double sfac = dold < 0.98 ? (1.0 - dam) / (1.0 - dold) : 0.0;
+                s0 *= sfac; s1 *= sfac; s2 *= sfac; s3 *= sfac;
+                ste2s *= sfac;
+            }
+        }
+    }
+    c.f.e_ste[p] = s0; PLN(c.f.e_ste, 1)[p] = s1; PLN(c.f.e_ste, 2)[p] = s2; PLN(c.f.e_ste, 3)[p] = s3;
+    c.f.e_ste2s[p] = ste2s;
+    c.f.e_sta2s[p] = sta2s;
+    c.f.e_tps[p] = tps;
+    c.f.e_dam[p] = dam;
+    c.f.e_strength[p] = strength;
+}
+
+// ============================================================ phase 8: vertex acceleration
+// calculate_acc_default / calculate_acc_pml (src/velocity.c:9-340): surface integral of
+// pressure + viscosity and deviatoric stress, hoop term, gravity and the nine-point
+// Laplacian damping (ANC); the PML form also integrates the auxiliary v_alpha.
+__global__ void k_vertex_acceleration(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!vert_active(c, i, j)) return;
+    const long long p = KIDX(i, j);
+    const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
+    const bool pml = (c.rp.damp_type == 1 || c.rp.damp_type == 2);
+    const double dt = c.scal->dt;
+    double ax = 0., ay = 0., vmass = 0., vvol = 0.;
+    double sub[4];
+    for (int k = 0; k < 4; ++k) sub[k] = PLN(c.f.v_subvol, k)[p];
+    double sigx = 0., sigy = 0.;
+    double alx = 0., aly = 0.;
+    if (pml) {
+        for (int k = 0; k < 4; ++k) { sigx += 0.25 * c.f.e_sigma[cl[k]]; sigy += 0.25 * PLN(c.f.e_sigma, 1)[cl[k]]; }
+        alx = c.f.v_alpha[p];
+        aly = PLN(c.f.v_alpha, 1)[p];
+    }
+    const bool damped = pml && (sigx > 0. || sigy > 0.);
+    for (int k = 0; k < 4; ++k) {
+        const long long e = cl[k];
+        const double sfx = PLN(c.f.v_suf, 2 * k)[p], sfy = PLN(c.f.v_suf, 2 * k + 1)[p];
+        const double lp = c.f.e_pre[e] + c.f.e_q[e];
+        const double ste0 = c.f.e_ste[e], ste1 = PLN(c.f.e_ste, 1)[e], ste2 = PLN(c.f.e_ste, 2)[e],
+                     ste3 = PLN(c.f.e_ste, 3)[e];
+        if (!pml) {
+            double fpx = 0., fpy = 0.;
+            fpx += lp * sfx;
+            fpy += lp * sfy;
+            fpx += sub[k] * lp;
+            const double sxx = ste0, szz = ste2, sxz = ste1, sth = ste3;
+            double fsx = 0., fsy = 0.;
+            fsx += sfx * sxx; fsx += sfy * sxz;
+            fsy += sfx * sxz; fsy += sfy * szz;
+            fsx += sub[k] * sth;
+            ax += -1.0 * fsx; ay += -1.0 * fsy;
+            ax += 1.0 * fpx; ay += 1.0 * fpy;
+        } else {
+            const double lpr = PLN(c.f.e_dampref, 2)[e];
+            double sxx = ste0 - lp, szz = ste2 - lp, sxz = ste1, sth = ste3 - lp;
+            double fsx = 0., fsy = 0.;
+            fsx += sfx * sxx; fsx += sfy * sxz;
+            fsy += sfx * sxz; fsy += sfy * szz;
+            fsx += sub[k] * sth;
+            ax += -1.0 * fsx; ay += -1.0 * fsy;
+            if (damped) {
+                sxx += lpr; szz += lpr; sth += lpr;
+                double t0 = 0.; t0 += sfx * (sigy * sxx); t0 += sfy * (sigx * sxz);
+                alx += t0 * dt;
+                double t1 = 0.; t1 += sfx * (sigy * sxz); t1 += sfy * (sigx * szz);
+                aly += t1 * dt;
+                alx += (sigx + sigy) * sub[k] * sth * dt;
+            }
+        }
+        const double lv = PLN(c.f.v_vol, 1 + k)[p];
+        vmass += lv * c.f.e_den[e];
+        vvol += lv;
+    }
+    if (damped) {
+        alx -= c.rp.alpha_damp_x * alx * dt;
+        aly -= c.rp.alpha_damp_y * aly * dt;
+        ax += -1.0 * alx; ay += -1.0 * aly;
+    }
+    if (pml) { c.f.v_alpha[p] = alx; PLN(c.f.v_alpha, 1)[p] = aly; }
+
+    double ancx = 0., ancy = 0.;
+    if (!vert_pad(c, i, j)) {
+        double lvx = 0., lvy = 0.;
+        int k = 0;
+        for (int dj = -1; dj <= 1; ++dj)
+            for (int di = -1; di <= 1; ++di, ++k) {
+                const long long q = KIDX(i + di, j + dj);
+                const double w = PLN(c.f.v_laplace, k)[p];
+                lvx += w * c.f.v_vel[q];
+                lvy += w * PLN(c.f.v_vel, 1)[q];
+            }
+        const double sc = 5.0e3 * sqrt(fabs(sub[0]) + fabs(sub[2]));
+        ancx = sc * lvx;
+        ancy = sc * lvy;
+    }
+    if (PLN(c.f.v_mass, 1)[p] >= 1.) { ancx = 0.; ancy = 0.; }
+    if (vmass > SALEC_TOLRHO * vvol) {
+        const double s = 1.0 / vmass;
+        ax *= s; ay *= s;
+        ax += 1.0 * c.f.v_bf[p]; ay += 1.0 * PLN(c.f.v_bf, 1)[p];
+        ax += c.rp.anc * ancx; ay += c.rp.anc * ancy;
+    } else if (pml) {
+        ax = c.f.v_bf[p]; ay = PLN(c.f.v_bf, 1)[p];
+    } else {
+        ax = 0.; ay = 0.;
+    }
+    if (fabs(ax) < c.rp.acceleration_min * 1) ax = 0.;
+    if (fabs(ay) < c.rp.acceleration_min * 1) ay = 0.;
+    c.f.v_acc[p] = ax;
+    PLN(c.f.v_acc, 1)[p] = ay;
+}
+
+// ============================================================ phase 9: vertex displacement
+// calculate_v_dis (src/sale2d.c:1238-1268).
+__global__ void k_vertex_displacement(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!vert_active(c, i, j)) return;
+    const long long p = KIDX(i, j);
+    const double dt = c.scal->dt;
+    const double hdt2 = 0.5 * dt * dt;
+    for (int k = 0; k < 2; ++k) {
+        const double v = PLN(c.f.v_vel, k)[p], a = PLN(c.f.v_acc, k)[p];
+        PLN(c.f.v_dis, k)[p] = dt * v + hdt2 * a;
+        PLN(c.f.v_vel, k)[p] = v + dt * a;
+    }
+}
+
+// ============================================================ phase 10: internal energy
+// update_energy (src/sale2d.c:564-712) with the Wunnemann porosity update.
+__global__ void k_energy(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!cell_interior(c, i, j)) return;
+    const long long p = KIDX(i, j);
+    const int nmat = c.d.nmat;
+    if (c.f.m_vof[p] > SALEC_TOLVOF || c.f.e_den[p] < SALEC_TOLRHO) return;
+    const double dt = c.scal->dt;
+    const double pre = c.f.e_pre[p];
+    const double lp = pre + c.f.e_q[p];
+    const double div = c.f.e_div_vel[p];
+    const double dE_pre = -lp * div;
+    const double g0 = c.f.e_grad_vel[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
+                 g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
+    const double dE_ste = c.f.e_ste[p] * g0 + PLN(c.f.e_ste, 1)[p] * (g1 + g2) + PLN(c.f.e_ste, 2)[p] * g3
+                        + PLN(c.f.e_ste, 3)[p] * g4;
+    double gam = 0.;
+    for (int m = 1; m < nmat; ++m) {
+        const double vm = PLN(c.f.m_vof, m)[p];
+        if (vm > SALEC_TOLVOF) gam += vm * c.mat[m].gamfrac / PLN(c.f.m_den, m)[p];
+    }
+    const double dcvs = div - gam * (dE_pre + dE_ste);
+    const double cvs = c.rp.porosity_model ? c.f.e_cvs[p] : 0.0;
+    for (int m = 1; m < nmat; ++m) {
+        const double vm = PLN(c.f.m_vof, m)[p];
+        const double rm = PLN(c.f.m_den, m)[p];
+        double *em = PLN(c.f.m_eng, m) + p;
+        if (vm <= SALEC_TOLVOF || rm <= SALEC_TOLRHO) {
+            *em = 0.;
+            if (c.rp.porosity_model) PLN(c.f.m_pty, m)[p] = 1.;
+        } else {
+            const double fac = 1.0;
+            *em = dmax(0., *em + (dE_pre + dE_ste) * dt * fac);
+            if (c.rp.porosity_model) {
+                double *pt = PLN(c.f.m_pty, m) + p;
+                double dpty = 0.;
+                if (c.f.e_sigma[p] + PLN(c.f.e_sigma, 1)[p] <= 0.) {
+                    double pa[6] = {*pt, cvs, pre, dcvs, c.f.e_vel[p], PLN(c.f.e_vel, 1)[p]};
+                    dpty = strength_fn(c.mat[m].porfunc, pa, c.mat[m]);
+                }
+                *pt += dpty * dt;
+                *pt = wind(*pt, 1.0, c.mat[m].alphamax2);
+            }
+        }
+    }
+    // the reference updates e_cvs for every non-vacuum cell, with or without porosity
+    c.f.e_cvs[p] = wind(c.f.e_cvs[p] + dcvs * dt, -10.0, 10.0);
+}
+
+// ============================================================ phase 12: face flux volumes
+// calculate_flux_mixed (src/advect.c:861-1136) with _calculate_flux_set_bphi (:1138-1223):
+// swept face volumes, geometric cut-line reconstruction of the primary material, algebraic
+// (MSTACS) fractions of the others, and the upwind state written on each outflow face.
+// A face with zero swept volume gets zero material volumes, which stands in for the
+// reference's clean_flux (src/advect.c:597-626): the other members of such a record are only
+// ever multiplied by those zero volumes.
+__device__ __forceinline__ double swept_volume(double xa, double ya, double xb, double yb, double dxa,
+                                               double dya, double dxb, double dyb)
+{
+    // get_flux_volcyl (src/advect.c:1347-1354)
+    const double x1 = -1.0 * dxa, y1 = -1.0 * dya, x2 = -1.0 * dxb, y2 = -1.0 * dyb;
+    const double vol = x1 * (ya - yb - y2) + x2 * (ya - yb + y1) + (y1 + y2) * (xb - xa);
+    return vol * fabs(2.0 * xa + 2.0 * xb + x1 + x2) / 8.0;
+}
+
+__device__ __forceinline__ double face_ratio(double p1, double p2)
+{
+    // geometric_flux_ratio (src/advect.c:1312-1330)
+    double a = p1, b = p2;
+    if (b > a) { a = p2; b = p1; }
+    if (b >= 0.0) return 1.0;
+    if (a <= 0.0) return 0.0;
+    return a / (a + fabs(b));
+}
+
+__device__ __forceinline__ double cut_length(double vf, double a, double b)
+{
+    // cut_length / cut_length_l / cut_length_s (src/advect.c:1356-1407)
+    if (a < b) { double t = a; a = b; b = t; }
+    if (1.0e-5 * a > b) {
+        double d;
+        if (vf <= 0.0) d = 0.0;
+        else if (vf <= 1.0) d = vf * a;
+        else d = a;
+        return d + b;
+    }
+    const double crf1 = 0.5 * b / a;
+    if (vf <= crf1) return sqrt(2.0 * a * b * vf);
+    if (vf <= 1.0 - crf1) return 0.5 * b + a * vf;
+    if (vf <= 1.0) return a + b - sqrt(2.0 * a * b * (1.0 - vf));
+    return a + b;
+}
+
+__device__ __forceinline__ void normalise2(double &x, double &y)
+{
+    // vec_norm (src/geometry/linear.c:132-146)
+    double len = 0.;
+    len += x * x;
+    len += y * y;
+    len = sqrt(len);
+    x /= len;
+    if (isnan(x)) x = 1.0;
+    y /= len;
+    if (isnan(y)) y = 1.0;
+}
+
+__device__ __forceinline__ double mstacs(double nd, double gf, double cr)
+{
+    // vofMSTACS (src/advect.c:1259-1274)
+    double cds, st;
+    if (cr < 1.0 / 3.0) cds = dmin(nd / cr, 1.0);
+    else cds = dmin(3.0 * nd, 1.0);
+    if (nd < 1.0 / 5.0) st = 3.0 * nd;
+    else if (nd < 1.0 / 2.0) st = (1.0 + nd) / 2.0;
+    else st = dmin((6.0 * nd + 3.0) / 8.0, 1.0);
+    return gf * cds + (1.0 - gf) * st;
+}
+
+__device__ __forceinline__ double algebraic_ratio(double vu, double vd, double va, double cr, double nx, double ny,
+                                                  double gx, double gy)
+{
+    // algebraic_flux_ratio (src/advect.c:1226-1253)
+    const double tmp = va - vu;
+    const double nd = (vd - vu) / tmp;
+    if (fabs(tmp) < SALEC_TOLVOF) return vd;
+    if (nd < SALEC_TOLVOF || nd > 1.0 - SALEC_TOLVOF) return vd;
+    double dot = 0.; dot += gx * nx; dot += gy * ny;
+    double len = 0.; len += gx * gx; len += gy * gy;
+    double cost = dot / sqrt(len);
+    cost = cost * cost;
+    const double gf = dmin(SALEC_CISSAMK1 * cost * cost, 1.0);
+    return vu + mstacs(nd, gf, cr) * (va - vu);
+}
+
+// pass 0: interior cells; pass 1: pad cells (after the ghost fills of m_den, m_eng, ...).
+__global__ void k_flux(const Ctx c, int pass)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= c.d.enx || j >= c.d.eny) return;
+    const bool interior = cell_interior(c, i, j);
+    if ((pass == 0) != interior) return;
+    const int nmat = c.d.nmat;
+    const long long p = KIDX(i, j);
+    const long long vl[4] = {KIDX(i, j), KIDX(i + 1, j), KIDX(i + 1, j + 1), KIDX(i, j + 1)};
+    double px[4], py[4], dx[4], dy[4];
+    for (int k = 0; k < 4; ++k) {
+        px[k] = c.f.v_pos[vl[k]]; py[k] = PLN(c.f.v_pos, 1)[vl[k]];
+        dx[k] = c.f.v_dis[vl[k]]; dy[k] = PLN(c.f.v_dis, 1)[vl[k]];
+    }
+    const double lv = swept_volume(px[0], py[0], px[3], py[3], dx[0], dy[0], dx[3], dy[3]);
+    const double rv = swept_volume(px[2], py[2], px[1], py[1], dx[2], dy[2], dx[1], dy[1]);
+    const double bv = swept_volume(px[1], py[1], px[0], py[0], dx[1], dy[1], dx[0], dy[0]);
+    const double uv = swept_volume(px[3], py[3], px[2], py[2], dx[3], dy[3], dx[2], dy[2]);
+    const double lbru[4] = {lv, bv, rv, uv};
+
+    double vof[SALEC_MAXMAT];
+    for (int m = 0; m < nmat; ++m) vof[m] = PLN(c.f.m_vof, m)[p];
+    const double evol = c.f.e_vol[p];
+    double flux[SALEC_MAXMAT][4];
+    for (int m = 0; m < nmat; ++m) flux[m][0] = flux[m][1] = flux[m][2] = flux[m][3] = 0.;
+
+    int prim = 0;
+    if (vof[0] < SALEC_TOLVOF)
+        for (int m = 1; m < nmat; ++m)
+            if (vof[m] > vof[prim]) prim = m;
+
+    double wpt[4];
+    if (vof[prim] > 1.0 - SALEC_TOLVOF) {
+        flux[prim][0] = dmin(lv, 0);
+        flux[prim][2] = -1.0 * dmin(rv, 0);
+        flux[prim][1] = dmin(bv, 0);
+        flux[prim][3] = -1.0 * dmin(uv, 0);
+        const double w = prim == 0 ? 1.0 : -0.25;
+        wpt[0] = wpt[1] = wpt[2] = wpt[3] = w;
+    } else {
+        double grd[12];
+        for (int k = 0; k < 8; ++k) grd[k] = PLN(c.f.e_grad, k)[p];
+        double gx = 0., gy = 0.;
+        {
+            const double *vv = PLN(c.f.v_vof, prim);
+            double vq[4];
+            for (int k = 0; k < 4; ++k) vq[k] = vv[vl[k]];
+            for (int k = 0; k < 4; ++k) gx += vq[k] * grd[k];
+            for (int k = 0; k < 4; ++k) gy += vq[k] * grd[4 + k];
+        }
+        normalise2(gx, gy);
+        double ca = PLN(c.f.e_pos, 2)[p] * fabs(gx);
+        double cb = PLN(c.f.e_pos, 3)[p] * fabs(gy);
+        if (ca < cb) { double t = ca; ca = cb; cb = t; }
+        const double dstar = cut_length(vof[prim], ca, cb);
+        double lw[4];
+        for (int k = 0; k < 4; ++k) { double s = 0.; s += gx * px[k]; s += gy * py[k]; lw[k] = s; }
+        const double mw = dmax(dmax(lw[0], lw[1]), dmax(lw[2], lw[3]));
+        for (int k = 0; k < 4; ++k) lw[k] = lw[k] - mw + dstar;
+        if (prim == 0) { for (int k = 0; k < 4; ++k) wpt[k] = lw[k]; }
+        else wpt[0] = wpt[1] = wpt[2] = wpt[3] = -0.25;
+        double fp[4];
+        fp[0] = face_ratio(lw[3], lw[0]);
+        fp[2] = face_ratio(lw[2], lw[1]);
+        fp[1] = face_ratio(lw[0], lw[1]);
+        fp[3] = face_ratio(lw[3], lw[2]);
+        double cr = dmin(lv, 0.0) + dmin(rv, 0) + dmin(bv, 0) + dmin(uv, 0);
+        cr = fabs(cr) / evol;
+        // neighbours l, b, r, u (the cell itself where the neighbour is off the mesh)
+        long long nb[4] = {KIDX(i - 1, j), KIDX(i, j - 1), KIDX(i + 1, j), KIDX(i, j + 1)};
+        if (i - 1 < 0) nb[0] = p;
+        if (j - 1 < 0) nb[1] = p;
+        if (i + 1 >= c.d.enx) nb[2] = p;
+        if (j + 1 >= c.d.eny) nb[3] = p;
+        // face normals l, b, r, u
+        const long long fb[4] = {KIDX(i, j), KIDX(i, j), KIDX(i + 1, j), KIDX(i, j + 1)};
+        double fnx[4], fny[4];
+        fnx[0] = c.f.bx_normal[fb[0]]; fny[0] = PLN(c.f.bx_normal, 1)[fb[0]];
+        fnx[2] = c.f.bx_normal[fb[2]]; fny[2] = PLN(c.f.bx_normal, 1)[fb[2]];
+        fnx[1] = c.f.by_normal[fb[1]]; fny[1] = PLN(c.f.by_normal, 1)[fb[1]];
+        fnx[3] = c.f.by_normal[fb[3]]; fny[3] = PLN(c.f.by_normal, 1)[fb[3]];
+        double fnp[SALEC_MAXMAT][4];
+        double snp[4] = {0., 0., 0., 0.};
+        for (int m = 0; m < nmat; ++m) fnp[m][0] = fnp[m][1] = fnp[m][2] = fnp[m][3] = 0.;
+        for (int m = 1; m < nmat; ++m) {
+            if (m == prim) continue;
+            const double *vv = PLN(c.f.v_vof, m);
+            double vq[4];
+            for (int k = 0; k < 4; ++k) vq[k] = vv[vl[k]];
+            double ngx = 0., ngy = 0.;
+            for (int k = 0; k < 4; ++k) ngx += vq[k] * grd[k];
+            for (int k = 0; k < 4; ++k) ngy += vq[k] * grd[4 + k];
+            normalise2(ngx, ngy);
+            const double *ev = PLN(c.f.m_vof, m);
+            const double up[4] = {ev[nb[0]], ev[nb[1]], ev[nb[2]], ev[nb[3]]};
+            const double ac[4] = {up[2], up[3], up[0], up[1]};
+            for (int k = 0; k < 4; ++k) {
+                fnp[m][k] = algebraic_ratio(up[k], vof[m], ac[k], cr, fnx[k], fny[k], ngx, ngy);
+                snp[k] += fnp[m][k];
+            }
+        }
+        for (int k = 0; k < 4; ++k) {
+            if (snp[k] > SALEC_TOLVOF) {
+                for (int m = 1; m < nmat; ++m) fnp[m][k] = fnp[m][k] / snp[k];
+            } else {
+                for (int m = 1; m < nmat; ++m) fnp[m][k] = vof[m] / (1.0 - vof[prim]);
+            }
+        }
+        for (int m = 0; m < nmat; ++m) {
+            if (m == prim) {
+                flux[m][0] = dmin(lv, 0.0) * fp[0];
+                flux[m][2] = -1.0 * dmin(rv, 0.0) * fp[2];
+                flux[m][1] = dmin(bv, 0.0) * fp[1];
+                flux[m][3] = -1.0 * dmin(uv, 0.0) * fp[3];
+            } else {
+                flux[m][0] = dmin(lv, 0.0) * (1.0 - fp[0]) * fnp[m][0];
+                flux[m][2] = -1.0 * dmin(rv, 0.0) * (1.0 - fp[2]) * fnp[m][2];
+                flux[m][1] = dmin(bv, 0.0) * (1.0 - fp[1]) * fnp[m][1];
+                flux[m][3] = -1.0 * dmin(uv, 0.0) * (1.0 - fp[3]) * fnp[m][3];
+            }
+        }
+    }
+    for (int k = 0; k < 4; ++k) PLN(c.f.e_wpt, k)[p] = wpt[k];
+
+    // cap the out-flux of each material by its content
+    for (int m = 1; m < nmat; ++m) {
+        double d = 0.;
+        d += flux[m][0] * 1.0; d += flux[m][1] * 1.0; d += flux[m][2] * -1.0; d += flux[m][3] * -1.0;
+        const double out = -1.0 * d;
+        if (out > vof[m] * evol) {
+            const double s = vof[m] * evol / out;
+            for (int k = 0; k < 4; ++k) flux[m][k] *= s;
+        }
+    }
+
+    // faces l, b, r, u
+    const long long PL = c.d.PL;
+    double *face[4] = {c.f.bx_phi + KIDX(i, j), c.f.by_phi + KIDX(i, j), c.f.bx_phi + KIDX(i + 1, j),
+                       c.f.by_phi + KIDX(i, j + 1)};
+    const int phi = c.d.phi;
+    for (int k = 0; k < 4; ++k) {
+        if (lbru[k] > 0.) continue;
+        double *f = face[k];
+        if (lbru[k] == 0.) {
+            for (int m = 0; m < nmat; ++m) f[m * PL] = 0.0;
+            continue;
+        }
+        for (int m = 0; m < nmat; ++m) {
+            f[m * PL] = flux[m][k];
+            f[(m + nmat) * PL] = PLN(c.f.m_den, m)[p];
+            f[(m + 2 * nmat) * PL] = PLN(c.f.m_eng, m)[p];
+        }
+        const int b = 3 * nmat;
+        f[(b + 0) * PL] = c.f.e_vel[p];
+        f[(b + 1) * PL] = PLN(c.f.e_vel, 1)[p];
+        for (int q = 0; q < 4; ++q) f[(b + 2 + q) * PL] = 1.0 * PLN(c.f.e_ste, q)[p];
+        f[(b + 6) * PL] = 1.0 * c.f.e_dam[p];
+        f[(b + 7) * PL] = 1.0 * c.f.e_tps[p];
+        f[(b + 8) * PL] = 1.0 * c.f.e_vib[p];
+        f[(b + 9) * PL] = 1.0 * c.f.e_ejt[p];
+        if (c.rp.porosity_model) {
+            f[(b + 10) * PL] = 1.0 * c.f.e_cvs[p];
+            for (int m = 0; m < nmat; ++m) f[(b + 11 + m) * PL] = PLN(c.f.m_pty, m)[p];
+        }
+        (void)phi;
+    }
+}
+
+// ============================================================ phase 14: remap + damping + EOS
+// advect_flux_default (src/advect.c:26-302), damp_on_cell (src/velocity.c:356-767),
+// ejecta_flow (src/ejecta.c:65-133) and update_state (src/sale2d.c:1635-1742), fused per cell:
+// the damping reads only its own cell, and the EOS reads the damped material state.
+__device__ void remap_cell(const Ctx &c, int i, int j, long long p)
+{
+    const int nmat = c.d.nmat;
+    const int phi = c.d.phi;
+    const long long PL = c.d.PL;
+    const bool por = c.rp.porosity_model != 0;
+    const double *face[4] = {c.f.bx_phi + KIDX(i, j), c.f.by_phi + KIDX(i, j), c.f.bx_phi + KIDX(i + 1, j),
+                             c.f.by_phi + KIDX(i, j + 1)};
+    const double dir[4] = {1.0, 1.0, -1.0, -1.0};
+    double dphi[4 * SALEC_MAXMAT + 11];
+    for (int q = 0; q < phi; ++q) dphi[q] = 0.;
+    const int b = 3 * nmat;
+    for (int k = 0; k < 4; ++k) {
+        const double *f = face[k];
+        for (int m = 0; m < nmat; ++m) {
+            const double mv = dir[k] * f[m * PL];
+            if (mv == 0.0) continue;   // adds only signed zeros to dphi (see k_flux)
+            const double rho_f = f[(m + nmat) * PL];
+            dphi[m] += mv;
+            dphi[m + nmat] += mv * rho_f;
+            dphi[m + 2 * nmat] += mv * f[(m + 2 * nmat) * PL];
+            const double fm = mv * rho_f;
+            for (int q = 0; q < 10; ++q) dphi[b + q] += fm * f[(b + q) * PL];
+            if (por) {
+                dphi[b + 10] += (f[(b + 10) * PL]) * (mv * rho_f);
+                dphi[m + b + 11] += (f[(m + b + 11) * PL]) * (mv * rho_f);
+            }
+        }
+    }
+    double vof[SALEC_MAXMAT], rho[SALEC_MAXMAT], eng[SALEC_MAXMAT], pty[SALEC_MAXMAT];
+    for (int m = 0; m < nmat; ++m) {
+        vof[m] = PLN(c.f.m_vof, m)[p];
+        rho[m] = PLN(c.f.m_den, m)[p];
+        eng[m] = PLN(c.f.m_eng, m)[p];
+        pty[m] = por ? PLN(c.f.m_pty, m)[p] : 1.0;
+    }
+    const double evol = c.f.e_vol[p];
+    double emass = evol * c.f.e_den[p];
+    double sphi[4 * SALEC_MAXMAT + 11];
+    for (int q = 0; q < phi; ++q) sphi[q] = 0.;
+    for (int m = 0; m < nmat; ++m) {
+        sphi[m] += vof[m] * evol;
+        sphi[m + nmat] += vof[m] * evol * rho[m];
+        sphi[m + 2 * nmat] += vof[m] * evol * eng[m];
+    }
+    for (int q = 0; q < 4; ++q) sphi[b + 2 + q] += emass * PLN(c.f.e_ste, q)[p];
+    sphi[b + 6] = emass * c.f.e_dam[p];
+    sphi[b + 7] = emass * c.f.e_tps[p];
+    sphi[b + 8] = emass * c.f.e_vib[p];
+    sphi[b + 9] = emass * c.f.e_ejt[p];
+    if (por) {
+        sphi[b + 10] = emass * c.f.e_cvs[p];
+        for (int m = 0; m < nmat; ++m) sphi[b + 11 + m] = vof[m] * evol * rho[m] * pty[m];
+    }
+    for (int q = 0; q < phi; ++q) sphi[q] += 1.0 * dphi[q];
+    double zeta = 0.0;
+    emass = 0.;
+    for (int m = 0; m < nmat; ++m) {
+        if (sphi[m] < 0.) { sphi[m] = 0.; sphi[m + nmat] = 0.; }
+        if (m == 0) continue;
+        zeta += sphi[m];
+        emass += sphi[m + nmat];
+    }
+    if (zeta > evol * (1.0 - SALEC_TOLVOF) || (zeta > 0. && sphi[0] < evol * SALEC_TOLVOF)) {
+        const double s = 1.0 / zeta;
+        for (int m = 0; m < nmat; ++m) vof[m] = s * sphi[m];
+        vof[0] = 0.0;
+    } else if (zeta < evol * SALEC_TOLVOF) {
+        for (int m = 0; m < nmat; ++m) vof[m] = 0.;
+        vof[0] = 1.0;
+    } else if (c.rp.partpres) {
+        const double s = 1.0 / (zeta + sphi[0]);
+        for (int m = 0; m < nmat; ++m) vof[m] = s * sphi[m];
+    } else {
+        sphi[0] = evol - zeta;
+        const double s = 1.0 / evol;
+        for (int m = 0; m < nmat; ++m) vof[m] = s * sphi[m];
+    }
+    for (int m = 1; m < nmat; ++m) {
+        if (vof[m] < SALEC_TOLVOF || sphi[m + nmat] < SALEC_TOLRHO * SALEC_TOLVOF * evol) {
+            eng[m] = 0.0; rho[m] = 0.0; vof[m] = 0.0;
+            if (por) pty[m] = 1.0;
+        } else {
+            eng[m] = sphi[m + 2 * nmat] / (vof[m] * evol);
+            rho[m] = sphi[m + nmat] / (vof[m] * evol);
+            if (por) pty[m] = sphi[b + 11 + m] / sphi[m + nmat];
+        }
+    }
+    double dvx, dvy, st[4], dam, tps, vib, ejt, cvs = por ? c.f.e_cvs[p] : 0.0;
+    if (emass > SALEC_TOLRHO * evol) {
+        const double s = 1.0 / emass;
+        dvx = s * sphi[b]; dvy = s * sphi[b + 1];
+        for (int q = 0; q < 4; ++q) st[q] = s * sphi[b + 2 + q];
+        dam = sphi[b + 6] / emass;
+        tps = sphi[b + 7] / emass;
+        vib = sphi[b + 8] / emass;
+        ejt = sphi[b + 9] / emass;
+        if (por) cvs = sphi[b + 10] / emass;
+    } else {
+        dvx = dvy = 0.;
+        st[0] = st[1] = st[2] = st[3] = 0.;
+        dam = tps = vib = ejt = 0.;
+        if (por) cvs = 0.;
+    }
+    double eden = emass / evol;
+    tps = wind(tps, 0.0, 10.0);
+    dam = wind(dam, 0.0, 1.0);
+    ejt = wind(ejt, 0.0, 1.0);
+    if (por)
+        for (int m = 1; m < nmat; ++m) pty[m] = wind(pty[m], 1.0, c.mat[m].alphamax2);
+    if (eden < c.rp.density_cutoff || eden < 10.0 * c.rp.density_cutoff * (1.0 - vof[0])) {
+        for (int m = 0; m < nmat; ++m) { vof[m] = 0.; rho[m] = 0.; eng[m] = 0.; }
+        vof[0] = 1.0;
+        dvx = dvy = 0.;
+        st[0] = st[1] = st[2] = st[3] = 0.;
+        dam = tps = vib = ejt = 0.;
+        if (por) {
+            cvs = 0.;
+            for (int m = 1; m < nmat; ++m) pty[m] = 1.0;
+        }
+    }
+    for (int m = 0; m < nmat; ++m) {
+        PLN(c.f.m_vof, m)[p] = vof[m];
+        PLN(c.f.m_den, m)[p] = rho[m];
+        PLN(c.f.m_eng, m)[p] = eng[m];
+        if (por) PLN(c.f.m_pty, m)[p] = pty[m];
+    }
+    c.f.e_dvel[p] = dvx;
+    PLN(c.f.e_dvel, 1)[p] = dvy;
+    for (int q = 0; q < 4; ++q) PLN(c.f.e_ste, q)[p] = st[q];
+    c.f.e_dam[p] = dam;
+    c.f.e_tps[p] = tps;
+    c.f.e_vib[p] = vib;
+    c.f.e_ejt[p] = ejt;
+    if (por) c.f.e_cvs[p] = cvs;
+    c.f.e_den[p] = eden;
+}
+
+__device__ void damp_cell(const Ctx &c, long long p, double dt)
+{
+    const int nmat = c.d.nmat;
+    const int ty = c.rp.damp_type;
+    if (ty == 4 || ty == 5) return;
+    if (c.f.m_vof[p] > SALEC_TOLVOF) return;
+    const double sx = c.f.e_sigma[p], sy = PLN(c.f.e_sigma, 1)[p];
+    const double d0 = c.f.e_dampref[p], d1 = PLN(c.f.e_dampref, 1)[p];
+    const bool por = c.rp.porosity_model != 0;
+    if (ty == 0) {
+        // damp_on_cell_pml (src/velocity.c:378-467)
+        double ax = c.f.e_alpha[p], ay = PLN(c.f.e_alpha, 1)[p];
+        const double pre = c.f.e_pre[p];
+        if (sy > 0.0) {
+            ay += (sy * PLN(c.f.e_grad_vel, 0)[p] + sy * PLN(c.f.e_grad_vel, 4)[p] - c.rp.alpha_damp_y * ay) * dt;
+            PLN(c.f.e_dvel, 1)[p] += -1.0 * sy * PLN(c.f.e_vel, 1)[p] * dt;
+            for (int m = 1; m < nmat; ++m) {
+                if (PLN(c.f.m_vof, m)[p] < 1.0 - SALEC_TOLVOF) continue;
+                double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
+                const double pt = por ? PLN(c.f.m_pty, m)[p] : 1.0;
+                const double rd = (-sy * (*rm - d0) - d0 * ay) * dt;
+                const double ed = (-sy * (*em - d1) - pre * ay) * dt;
+                *rm += rd / pt;
+                *em += ed / pt;
+                break;
+            }
+        }
+        if (sx > 0.0) {
+            ax += (sx * PLN(c.f.e_grad_vel, 3)[p] + sx * PLN(c.f.e_grad_vel, 4)[p] - c.rp.alpha_damp_x * ax) * dt;
+            c.f.e_dvel[p] += -1.0 * sx * c.f.e_vel[p] * dt;
+            for (int m = 1; m < nmat; ++m) {
+                if (PLN(c.f.m_vof, m)[p] > 1.0 - SALEC_TOLVOF) {
+                    double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
+                    const double pt = por ? PLN(c.f.m_pty, m)[p] : 1.0;
+                    const double rd = (-sx * (*rm - d0) - d0 * (ax + ay)) * dt;
+                    const double ed = (-sx * (*em - d1) - pre * (ax + ay)) * dt;
+                    *rm += rd / pt;
+                    *em += ed / pt;
+                    break;
+                }
+            }
+        }
+        c.f.e_alpha[p] = ax;
+        PLN(c.f.e_alpha, 1)[p] = ay;
+    } else if (ty == 1 || ty == 2) {
+        // damp_on_cell_pml2 / _pml3 (src/velocity.c:471-654)
+        if (!(sy > 0.0 || sx > 0.0)) return;
+        const double ss = sx + sy;
+        c.f.e_dvel[p] += -1.0 * ss * c.f.e_vel[p] * dt;
+        PLN(c.f.e_dvel, 1)[p] += -1.0 * ss * PLN(c.f.e_vel, 1)[p] * dt;
+        double ax = c.f.e_alpha[p], ay = PLN(c.f.e_alpha, 1)[p];
+        const double g0 = PLN(c.f.e_grad_vel, 0)[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
+                     g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
+        const double adx = c.rp.alpha_damp_x, ady = c.rp.alpha_damp_y;
+        ax += (sy * g0 + sy * g4 - ady * ax) * dt + (sx * g3 + sx * g4 - adx * ax) * dt;
+        const double lp = c.f.e_pre[p] + c.f.e_q[p] - PLN(c.f.e_dampref, 2)[p];
+        const double t0 = c.f.e_ste[p], t1 = PLN(c.f.e_ste, 1)[p], t2 = PLN(c.f.e_ste, 2)[p], t3 = PLN(c.f.e_ste, 3)[p];
+        const double sd = (t0 - lp) * sy * g0 + t1 * (sy * g1 + sx * g2) + (t2 - lp) * sx * g3 + (sy + sx) * t3 * g4;
+        ay += -1.0 * sd * dt - 1.0 * (adx + ady) * ay * dt;
+        c.f.e_alpha[p] = ax;
+        PLN(c.f.e_alpha, 1)[p] = ay;
+        for (int m = 1; m < nmat; ++m) {
+            if (PLN(c.f.m_vof, m)[p] < 1.0 - SALEC_TOLVOF) continue;
+            double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
+            if (ty == 1) {
+                const double pt = por ? PLN(c.f.m_pty, m)[p] : 1.0;
+                const double rd = (-(sx + sy) * (*rm - d0) - d0 * ax) * dt;
+                const double ed = (-(sx + sy) * (*em - d1) - ay) * dt;
+                *rm += rd / pt;
+                *em += ed / pt;
+            } else {
+                const double rd = (-(sx + sy) * (*rm - d0)) * dt;
+                const double ed = (-(sx + sy) * (*em - d1) - ay) * dt;
+                *rm += rd;
+                *em += ed;
+            }
+            break;
+        }
+    } else if (ty == 3) {
+        // damp_on_cell_sbc (src/velocity.c:658-767); "+=" in y and "=" in x as in the reference
+        if (sy < 1.0) {
+            for (int m = 1; m < nmat; ++m) {
+                if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
+                double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
+                const double dd = *rm - d0, de = *em - d1;
+                *rm += dd * sy + d0;
+                *em += de * sy + d1;
+            }
+        }
+        if (sx < 1.0) {
+            for (int m = 1; m < nmat; ++m) {
+                if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
+                double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
+                const double dd = *rm - d0, de = *em - d1;
+                *rm = dd * sx + d0;
+                *em = de * sx * sx + d1;
+            }
+        }
+    }
+}
+
+__device__ void ejecta_drag_cell(const Ctx &c, int i, int j, long long p, double dt)
+{
+    // ejecta_flow (src/ejecta.c:65-133); inactive unless resistance or friction is positive
+    const double ey = PLN(c.f.e_pos, 1)[p];
+    const double gy = 0.5 * PLN(c.f.v_bf, 1)[KIDX(i - 1, j - 1)] + 0.5 * PLN(c.f.v_bf, 1)[KIDX(i, j - 1)];
+    double gyy = 0.;
+    gyy += gy;
+    if (ey <= c.f.y_profile[i] && c.f.e_ejt[p] > 0.1) {
+        if (c.rp.flow_resistance > 0.) {
+            c.f.e_dvel[p] += -c.rp.flow_resistance * dt * c.f.e_vel[p];
+            PLN(c.f.e_dvel, 1)[p] += -c.rp.flow_resistance * dt * PLN(c.f.e_vel, 1)[p];
+        }
+        if (c.rp.flow_friction > 0.) {
+            for (int q = 0; q < 4; ++q) PLN(c.f.e_ste, q)[p] = 0.;
+            if (c.f.e_vel[p] >= 0.) c.f.e_dvel[p] += -1.0 * c.rp.flow_friction * fabs(gyy) * dt;
+            else c.f.e_dvel[p] += 1.0 * c.rp.flow_friction * fabs(gyy) * dt;
+        }
+    }
+}
+
+__device__ void state_cell(const Ctx &c, long long p)
+{
+    const int nmat = c.d.nmat;
+    const bool por = c.rp.porosity_model != 0;
+    const double dam = c.f.e_dam[p];
+    double mpre[SALEC_MAXMAT], mcsd[SALEC_MAXMAT], mtem[SALEC_MAXMAT];
+    double epre = 0.0, ecsd = 0.0, etem = 0.0, eden = 0.0, emu = 0.0;
+    for (int m = 1; m < nmat; ++m) {
+        const double vm = PLN(c.f.m_vof, m)[p];
+        if (vm < SALEC_TOLVOF) {
+            mpre[m] = 0.; mcsd[m] = 1.; mtem[m] = 0.;
+        } else {
+            const DevMat &s = c.mat[m];
+            const double plim = (1.0 - dam) * s.minPint + dam * s.minPdam;
+            const double pt = por ? PLN(c.f.m_pty, m)[p] : 1.0;
+            material_state(s, PLN(c.f.m_den, m)[p], PLN(c.f.m_eng, m)[p], plim, pt, mtem[m], mpre[m], mcsd[m]);
+        }
+    }
+    for (int m = 1; m < nmat; ++m) {
+        const double vm = PLN(c.f.m_vof, m)[p];
+        const double rm = PLN(c.f.m_den, m)[p];
+        epre += vm * mpre[m];
+        ecsd += vm / dmax(1.0, mcsd[m]);
+        etem += vm * mtem[m];
+        eden += vm * rm;
+        emu += vm / dmax(1.0, rm * mcsd[m] * mcsd[m] * c.mat[m].GaCoef);
+    }
+    if (emu > 0.) emu = 1.0 / emu;
+    if (ecsd > 0.) ecsd = 1.0 / ecsd;
+    const double v0 = c.f.m_vof[p];
+    if ((c.rp.partpres == 0 && v0 > SALEC_TOLVOF) || (c.rp.partpres == 1 && v0 > 1.0 - SALEC_TOLVOF)) {
+        epre = 0.;
+        ecsd = 1.0;
+        emu = 0.;
+    } else if (c.rp.partpres == 1) {
+        ecsd = ecsd * (1.0 - v0);
+        etem = etem / (1.0 - v0);
+        emu = emu * (1.0 - v0);
+    }
+    c.f.e_pre[p] = epre;
+    c.f.e_csd[p] = ecsd;
+    c.f.e_tem[p] = etem;
+    c.f.e_den[p] = eden;
+    c.f.e_mu[p] = emu;
+}
+
+__global__ void k_remap_damp_state(const Ctx c, int do_remap, int do_damp, int do_ejecta, int do_state)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= c.d.enx || j >= c.d.eny) return;
+    const long long p = KIDX(i, j);
+    const bool interior = cell_interior(c, i, j);
+    const double dt = c.scal->dt;
+    if (do_remap && interior) remap_cell(c, i, j, p);
+    if (do_damp && c.rp.damp_time > c.scal->time) damp_cell(c, p, dt);
+    if (do_ejecta && interior) ejecta_drag_cell(c, i, j, p, dt);
+    if (do_state && interior) state_cell(c, p);
+}
+
+// ============================================================ phase 15: cycle control
+// update_cycle_control (src/sale2d.c:71-136): advance time and step counter; seed the next
+// CFL reduction with 1.1 * dt (src/sale2d.c:1961).
+__global__ void k_cycle(const Ctx c)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        Scal *s = c.scal;
+        s->time += s->dt;
+        s->i_step += 1;
+        s->dt_acc = ord_encode(1.1 * s->dt);
+    }
+}
+
+// ============================================================ boundary gathers
+// Apply a precomputed gather map (built on the host from the reference's ghost and
+// restriction tables): dst[k] = op_c(src[k]) per component c. In-place when no source is also
+// a destination; otherwise gathered through scratch in two passes.
+__device__ __forceinline__ double apply_op(unsigned op, double v)
+{
+    switch (op) {
+    case 0: return v;
+    case 1: return -1.0 * v;
+    case 2: return fabs(v);
+    case 3: return -fabs(v);
+    default: return 0.0;
+    }
+}
+
+__global__ void k_gather(GatherBatch g, int mode, double *scratch)
+{
+    // mode 0: in place; 1: gather into scratch; 2: scatter from scratch
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.total) return;
+    int f = 0;
+    while (f + 1 < g.nfield && t >= g.start[f + 1]) ++f;
+    const GatherField &gf = g.field[f];
+    const int k = t - g.start[f];
+    const long long d = gf.dst[k], s = gf.src[k];
+    const unsigned ops = gf.ops[k];
+    for (int comp = 0; comp < gf.ncomp; ++comp) {
+        double *plane = gf.base + (long long)comp * gf.plane;
+        const unsigned op = (ops >> (3 * comp)) & 7u;
+        if (mode == 0) {
+            plane[d] = apply_op(op, plane[s]);
+        } else if (mode == 1) {
+            scratch[(long long)t * gf.ncomp_max + comp] = apply_op(op, plane[s]);
+        } else {
+            plane[d] = scratch[(long long)t * gf.ncomp_max + comp];
+        }
+    }
+}
+
+// ============================================================ layout conversion
+// Reference AoS block (points x-fastest, components innermost) <-> planes.
+__global__ void k_aos_to_planes(const double *aos, double *base, long long plane, int P, int nx, int ny, int nc)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)nx * ny;
+    if (t >= n) return;
+    const int i = (int)(t % nx), j = (int)(t / nx);
+    for (int k = 0; k < nc; ++k) base[(long long)k * plane + i + (long long)P * j] = aos[t * nc + k];
+}
+
+__global__ void k_planes_to_aos(const double *base, double *aos, long long plane, int P, int nx, int ny, int nc)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)nx * ny;
+    if (t >= n) return;
+    const int i = (int)(t % nx), j = (int)(t / nx);
+    for (int k = 0; k < nc; ++k) aos[t * nc + k] = base[(long long)k * plane + i + (long long)P * j];
+}
+
+__global__ void k_count_nonfinite(const double *base, long long n, unsigned long long *out)
+{
+    unsigned long long bad = 0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        if (!isfinite(base[t])) ++bad;
+    for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, o);
+    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(out, bad);
+}
+
+} // namespace salec

@@ -1,0 +1,218 @@
+"""ctypes mirror of include/salec_gpu.h: the host-side interface of the B200 mesh update.
+
+``Simulation`` owns one device handle. Fields cross the boundary in the reference's own
+layout and are exposed here as numpy arrays of shape (points_y, points_x, components), the
+shape of the reference's ``field_var.data`` viewed row by row.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+from . import build as _build
+
+c_d, c_i, c_ll = ctypes.c_double, ctypes.c_int, ctypes.c_longlong
+P_D = ctypes.POINTER(c_d)
+
+SALEC_OK = 0
+STATUS = {0: "SALEC_OK", -1: "SALEC_ERR_ARG", -2: "SALEC_ERR_CUDA", -3: "SALEC_ERR_ALLOC",
+          -4: "SALEC_ERR_STATE", -5: "SALEC_ERR_UNSUPPORTED", -6: "SALEC_ERR_NUMERIC"}
+EOS_ANEOS, EOS_TILLOTSON, EOS_SIEDEN = 0, 1, 2
+DAMP = {"pml": 0, "pml2": 1, "pml3": 2, "sbc": 3, "ctlg": 4, "none": 5}
+NPHASE = 16
+
+
+class RunDesc(ctypes.Structure):
+    _fields_ = [("nx", c_i), ("ny", c_i), ("nmat", c_i), ("damp_type", c_i), ("go", c_i * 4),
+                ("partpres", c_i), ("porosity_model", c_i), ("acoustic_fluid", c_i), ("tensile_failure", c_i),
+                ("tracer_lubrication", c_i), ("tracer_lub_gy0", c_i), ("tracer_lub_gy1", c_i),
+                ("avis1", c_d), ("avis2", c_d), ("anc", c_d),
+                ("density_cutoff", c_d), ("velocity_max", c_d), ("velocity_min", c_d), ("acceleration_min", c_d),
+                ("alpha_damp_x", c_d), ("alpha_damp_y", c_d), ("damp_time", c_d),
+                ("threshold_z", c_d), ("flow_resistance", c_d), ("flow_friction", c_d),
+                ("tracer_lub_y0", c_d), ("tracer_lub_frac", c_d),
+                ("max_dt", c_d), ("dt", c_d), ("time", c_d), ("i_step", c_i)]
+
+
+MAT_DOUBLES = ["VaporDen", "MeltDen", "GaCoef", "Yint0", "Yfricint", "Ylimint", "Ydam0", "Yfricdam", "Ylimdam",
+               "Yten0", "IvanA", "IvanB", "IvanC", "Pbd", "Pbp", "minPint", "minPdam", "JCA", "JCB", "JCN", "JCC",
+               "JCM", "JCTREF", "JCMaxPlastic", "Asimon", "Csimon", "Tmelt0", "Tfrac", "Tdelta"]
+MAT_DOUBLES2 = ["Tlidc1", "Tlidc2", "Tlidc3", "Tsolc1", "Tsolc2", "Tsolc3", "Toff", "Cvib", "VibMax", "Tdamp",
+                "Pvlim", "Acvis", "alpha0", "alphax", "epse0", "chi", "kappa", "avel", "epsec", "epsex",
+                "alphamax", "alphamax2", "alphae", "gamfrac", "melt_viscosity"]
+
+
+class MaterialDesc(ctypes.Structure):
+    _fields_ = ([("eos_type", c_i), ("yfunc", c_i), ("tfunc", c_i), ("dsdf", c_i), ("porfunc", c_i)]
+                + [(n, c_d) for n in MAT_DOUBLES]
+                + [("PolyLiq", c_i), ("PolySol", c_i)]
+                + [(n, c_d) for n in MAT_DOUBLES2]
+                + [("till", c_d * 13), ("cold_n", c_i), ("cold_xden", P_D), ("cold_yeng", P_D),
+                   ("ntem", c_i), ("nden", c_i), ("xtem", P_D), ("yden", P_D), ("data", P_D)])
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the in-tree library (building it first if it is missing or stale)."""
+    global _lib
+    if _lib is None:
+        path = _build.LIB
+        if not os.path.exists(path) or _build._stale():
+            try:
+                _build.build()
+            except Exception as e:  # no nvcc on this machine: only a prebuilt library can be used
+                if not os.path.exists(path):
+                    raise RuntimeError("libsalec_b200.so is missing and cannot be built: %s" % e)
+        L = ctypes.CDLL(path)
+        vp = ctypes.c_void_p
+        sig = {
+            "salec_gpu_create": ([ctypes.POINTER(RunDesc), ctypes.POINTER(MaterialDesc), ctypes.POINTER(vp)], c_i),
+            "salec_gpu_destroy": ([vp], c_i),
+            "salec_gpu_field_index": ([ctypes.c_char_p], c_i),
+            "salec_gpu_field_shape": ([vp, c_i, ctypes.POINTER(c_i), ctypes.POINTER(c_i), ctypes.POINTER(c_i)], c_i),
+            "salec_gpu_set_field": ([vp, c_i, P_D, c_ll], c_i),
+            "salec_gpu_get_field": ([vp, c_i, P_D, c_ll], c_i),
+            "salec_gpu_step": ([vp, c_i], c_i),
+            "salec_gpu_phases": ([vp, c_i, c_i], c_i),
+            "salec_gpu_sync": ([vp], c_i),
+            "salec_gpu_get_scalar": ([vp, ctypes.c_char_p, P_D], c_i),
+            "salec_gpu_set_scalar": ([vp, ctypes.c_char_p, c_d], c_i),
+            "salec_gpu_set_tracers": ([vp, c_i, P_D], c_i),
+            "salec_gpu_get_tracers": ([vp, P_D, ctypes.POINTER(c_i)], c_i),
+            "salec_gpu_check": ([vp, ctypes.POINTER(c_ll)], c_i),
+            "salec_gpu_func_index": ([ctypes.c_char_p], c_i),
+            "salec_gpu_last_error": ([], ctypes.c_char_p),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+class SalecError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        msg = lib().salec_gpu_last_error().decode(errors="replace")
+        super().__init__("%s failed: %s (%s)" % (what, STATUS.get(code, code), msg))
+        self.code = code
+
+
+def _check(code: int, what: str) -> None:
+    if code != SALEC_OK:
+        raise SalecError(code, what)
+
+
+def func_index(name: str) -> int:
+    k = lib().salec_gpu_func_index(name.encode())
+    if k < 0:
+        raise ValueError("unknown strength/damage/porosity function %r" % name)
+    return k
+
+
+def field_index(name: str) -> int:
+    k = lib().salec_gpu_field_index(name.encode())
+    if k < 0:
+        raise KeyError(name)
+    return k
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(P_D)
+
+
+class Simulation:
+    """One device-resident simulation (a salec_gpu handle)."""
+
+    def __init__(self, run: RunDesc, materials: Sequence[Dict]):
+        """``materials``: one dict per material index (entry 0, vacuum, may be empty) with the
+        MaterialDesc scalar fields plus ``till`` (13 values), ``cold_yeng`` (array) or
+        ``xtem``/``yden``/``data`` arrays for tabulated kinds."""
+        n = run.nmat
+        arr = (MaterialDesc * n)()
+        self._keep = []
+        for m in range(1, n):
+            spec = materials[m]
+            md = arr[m]
+            for k, v in spec.items():
+                if k in ("till",):
+                    for q in range(13):
+                        md.till[q] = float(v[q])
+                elif k in ("cold_yeng", "cold_xden", "xtem", "yden", "data"):
+                    a = np.ascontiguousarray(v, dtype=np.float64).ravel()
+                    self._keep.append(a)
+                    setattr(md, k, _ptr(a))
+                    if k == "cold_yeng":
+                        md.cold_n = a.size
+                else:
+                    setattr(md, k, v)
+        h = ctypes.c_void_p()
+        _check(lib().salec_gpu_create(ctypes.byref(run), arr, ctypes.byref(h)), "salec_gpu_create")
+        self.h = h
+        self.run = run
+
+    def close(self) -> None:
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().salec_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def shape(self, name: str):
+        nx, ny, nc = c_i(), c_i(), c_i()
+        _check(lib().salec_gpu_field_shape(self.h, field_index(name), ctypes.byref(nx), ctypes.byref(ny),
+                                           ctypes.byref(nc)), "field_shape")
+        return ny.value, nx.value, nc.value
+
+    def set_field(self, name: str, a: np.ndarray) -> None:
+        shp = self.shape(name)
+        b = np.ascontiguousarray(a, dtype=np.float64).reshape(shp)
+        _check(lib().salec_gpu_set_field(self.h, field_index(name), _ptr(b), b.size), "set_field " + name)
+
+    def get_field(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape(name), dtype=np.float64)
+        _check(lib().salec_gpu_get_field(self.h, field_index(name), _ptr(out), out.size), "get_field " + name)
+        return out
+
+    def step(self, n: int = 1) -> None:
+        _check(lib().salec_gpu_step(self.h, n), "step")
+
+    def phases(self, first: int, last: int) -> None:
+        _check(lib().salec_gpu_phases(self.h, first, last), "phases")
+
+    def sync(self) -> None:
+        _check(lib().salec_gpu_sync(self.h), "sync")
+
+    def scalar(self, name: str) -> float:
+        v = c_d()
+        _check(lib().salec_gpu_get_scalar(self.h, name.encode(), ctypes.byref(v)), "get_scalar " + name)
+        return v.value
+
+    def set_scalar(self, name: str, value: float) -> None:
+        _check(lib().salec_gpu_set_scalar(self.h, name.encode(), float(value)), "set_scalar " + name)
+
+    def check(self) -> int:
+        n = c_ll()
+        code = lib().salec_gpu_check(self.h, ctypes.byref(n))
+        if code not in (SALEC_OK, -6):
+            _check(code, "check")
+        return n.value
+
+    def set_tracers(self, rows: np.ndarray) -> None:
+        r = np.ascontiguousarray(rows, dtype=np.float64).reshape(-1, 12)
+        _check(lib().salec_gpu_set_tracers(self.h, r.shape[0], _ptr(r)), "set_tracers")
+
+    def get_tracers(self, capacity: int) -> np.ndarray:
+        out = np.zeros((max(capacity, 1), 12))
+        n = c_i(capacity)
+        _check(lib().salec_gpu_get_tracers(self.h, _ptr(out), ctypes.byref(n)), "get_tracers")
+        return out[: n.value]
