@@ -131,14 +131,29 @@ int salec_gpu_sync(salec_gpu *h);
 int salec_gpu_get_scalar(salec_gpu *h, const char *name, double *value);
 int salec_gpu_set_scalar(salec_gpu *h, const char *name, double value);
 
-/* Lagrangian tracers (src/tracer.c:52-175). Rows of 12 doubles per tracer:
- * x, y, vx, vy, mpre, mtem, gx, gy, tag, matid, cell_x, cell_y. get returns live tracers in
- * their original order; *n is in/out (capacity in, count out). */
+/* Lagrangian tracers (src/tracer.c:52-175, list built by fl_tracer_init :380-450). Rows of 12
+ * doubles per tracer: x, y, vx, vy, mpre, mtem, gx, gy, tag, matid, cell_x, cell_y (cell_x/y is
+ * the reference's node->id). set replaces the tracer list; get returns the live tracers in
+ * list order, *n is in/out (row capacity in, live count out); rows == NULL only counts. */
 int salec_gpu_set_tracers(salec_gpu *h, int n, const double *rows);
 int salec_gpu_get_tracers(salec_gpu *h, double *rows, int *n);
 
 /* Count non-finite values in the evolving cell and vertex fields; SALEC_ERR_NUMERIC if any. */
 int salec_gpu_check(salec_gpu *h, long long *n_bad);
+
+/*
+ * Boundary tables compiled to gather maps (host only, no device needed). The reference fills
+ * ghost cells and restricts boundary vertices by walking a table point by point
+ * (src/mpi_vec/mpi_vec_ght.c:279-357 and :657-696); the map gives, for each point the walk
+ * writes, the original point its final value comes from and a per-component transform
+ * (3 bits per component: 0 copy, 1 negate, 2 abs, 3 -abs, 4 +0, 5 -0).
+ * kind 0: ghost table of a cell field with pattern (0 always-copy, 1 normal, 2 velocity
+ * increment, 3 velocity, 4 stress, 5 density); kind 1: vertex restriction table.
+ * nx, ny: points of the field in x and y; points are indexed x-fastest. *n is in/out
+ * (capacity in, entries out); dst/src/ops may be NULL to query the count.
+ */
+int salec_boundary_map(int kind, int pattern, int nx, int ny, int ncomp, const int go[4], int *n, int *dst,
+                       int *src, unsigned *ops);
 
 /* Strength/damage/porosity function index for a reference name (case-insensitive), or -1. */
 int salec_gpu_func_index(const char *name);

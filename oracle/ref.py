@@ -49,6 +49,7 @@ def lib() -> ctypes.CDLL:
             "ref_get_table": ([c_i, pi, pi, pd, pd, pd], c_i),
             "ref_eos_state": ([c_i, c_d, c_d, c_d, c_d, pd], c_i),
             "ref_tracer_count": ([], c_i), "ref_get_tracers": ([pd], c_i),
+            "ref_ghost_fill": ([c_s], c_i), "ref_restrict": ([c_s], c_i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -171,6 +172,14 @@ def tracers() -> np.ndarray:
     out = np.zeros((max(n, 1), 12))
     m = lib().ref_get_tracers(_pd(out))
     return out[:m]
+
+
+def ghost_fill(name: str) -> None:
+    _check(lib().ref_ghost_fill(name.encode()), "ghost_fill " + name)
+
+
+def restrict(name: str) -> None:
+    _check(lib().ref_restrict(name.encode()), "restrict " + name)
 
 
 def write_output() -> None:

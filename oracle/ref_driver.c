@@ -337,6 +337,24 @@ int ref_set_field(const char *name, const double *in)
     return 0;
 }
 
+/* The reference's own boundary passes on one field: ghost fill (flush_ght,
+ * src/mpi_vec/mpi_vec_ght.c:736-752) or vertex restriction (sync_restrict_vertexes, :723-734). */
+int ref_ghost_fill(const char *name)
+{
+    field_var *fv = field_by_name(name);
+    if (!fv || g_stage < 1) return -1;
+    flush_ght(fv);
+    return 0;
+}
+
+int ref_restrict(const char *name)
+{
+    field_var *fv = field_by_name(name);
+    if (!fv || g_stage < 1) return -1;
+    sync_restrict_vertexes(fv);
+    return 0;
+}
+
 /* ----------------------------------------------------------------- scalars */
 
 int ref_get_scalar(const char *n, double *v)

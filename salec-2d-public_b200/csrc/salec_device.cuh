@@ -88,12 +88,22 @@ struct Fields {
     double *bx_phi, *by_phi, *bx_normal, *by_normal, *y_profile;
 };
 
+// Lagrangian tracers as structure-of-arrays in the reference's list order
+// (tracer_t of src/mpi_vec/linked_list.h:17-27 plus the cell index and a live flag).
+struct Tracers {
+    double *x, *y, *vx, *vy, *rec_pre, *rec_tem;
+    float *mpre, *mtem;
+    int *gx, *gy, *tag, *matid, *cx, *cy, *alive;
+    int n;
+};
+
 struct Ctx {
     Dims d;
     Fields f;
     RunParams rp;
     const DevMat *mat;
     Scal *scal;
+    Tracers tr;
 };
 
 // ------------------------------------------------------------------ small helpers

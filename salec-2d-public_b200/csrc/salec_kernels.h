@@ -56,6 +56,7 @@ __global__ void k_stress(const Ctx c);
 __global__ void k_vertex_acceleration(const Ctx c);
 __global__ void k_vertex_displacement(const Ctx c);
 __global__ void k_energy(const Ctx c);
+__global__ void k_tracers(const Ctx c);
 __global__ void k_flux(const Ctx c, int pass);
 __global__ void k_remap_damp_state(const Ctx c, int do_remap, int do_damp, int do_ejecta, int do_state);
 __global__ void k_cycle(const Ctx c);

@@ -111,7 +111,8 @@ struct salec_gpu {
     double *staging = nullptr;   // AoS staging for field transfer
     size_t staging_doubles = 0;
     Gather g_mvof, g_dvel_den, g_evel, g_pre_ste_q, g_flux_state, r_vel, r_acc, r_dis;
-    int ntracer = 0;
+    Tracers tr{};
+    void *tr_block = nullptr;   // one allocation holding every tracer array
 
     Ctx ctx() const
     {
@@ -121,6 +122,7 @@ struct salec_gpu {
         c.rp = rp;
         c.mat = mat;
         c.scal = scal;
+        c.tr = tr;
         return c;
     }
 };
@@ -251,7 +253,9 @@ int run_phase(salec_gpu *h, int ph)
         rc = run_gather(h, h->r_dis);
         break;
     case 10: k_energy<<<gc, blk, 0, s>>>(c); break;
-    case 11: break;   // tracers: see salec_tracer.cu
+    case 11:
+        if (h->tr.n > 0) k_tracers<<<(h->tr.n + 127) / 128, 128, 0, s>>>(c);
+        break;
     case 12:
         k_flux<<<gc, blk, 0, s>>>(c, 0);
         rc = run_gather(h, h->g_flux_state);
@@ -387,6 +391,7 @@ void release(salec_gpu *h)
     if (h->scal) cudaFree(h->scal);
     if (h->scal_host) cudaFreeHost(h->scal_host);
     if (h->mat) cudaFree(h->mat);
+    if (h->tr_block) cudaFree(h->tr_block);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -410,6 +415,24 @@ int salec_gpu_func_index(const char *name)
 }
 
 int salec_gpu_field_index(const char *name) { return field_by_name(name); }
+
+int salec_boundary_map(int kind, int pattern, int nx, int ny, int ncomp, const int go[4], int *n, int *dst,
+                       int *src, unsigned *ops)
+{
+    if (!go || !n || nx < 8 || ny < 8 || ncomp < 1 || ncomp > 10 || pattern < 0 || pattern > 5)
+        return fail(SALEC_ERR_ARG, "bad boundary map request");
+    GatherMap m;
+    if (kind == 0) m = build_ghost_map(nx, ny, nx, ncomp, go, (GhostPattern)pattern);
+    else if (kind == 1) m = build_restrict_map(nx, ny, nx, ncomp, go);
+    else return fail(SALEC_ERR_ARG, "kind must be 0 (ghost) or 1 (restrict)");
+    const int cnt = (int)m.dst.size();
+    if (dst && src && ops) {
+        if (*n < cnt) { *n = cnt; return fail(SALEC_ERR_ARG, "map buffer too small"); }
+        for (int k = 0; k < cnt; ++k) { dst[k] = m.dst[k]; src[k] = m.src[k]; ops[k] = m.ops[k]; }
+    }
+    *n = cnt;
+    return SALEC_OK;
+}
 
 int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats, salec_gpu **out)
 {
@@ -588,17 +611,83 @@ int salec_gpu_set_scalar(salec_gpu *h, const char *name, double value)
 
 int salec_gpu_set_tracers(salec_gpu *h, int n, const double *rows)
 {
-    (void)rows;
-    if (!h || n < 0) return fail(SALEC_ERR_ARG, "bad argument");
-    h->ntracer = n;
+    if (!h || n < 0 || (n > 0 && !rows)) return fail(SALEC_ERR_ARG, "bad argument");
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->tr_block) cudaFree(h->tr_block);
+    h->tr_block = nullptr;
+    h->tr = Tracers();
+    if (n == 0) return SALEC_OK;
+    const size_t nd = 6, nf = 2, ni = 7;
+    auto rounded = [](size_t sz) { return ((sz + 255) / 256) * 256; };
+    const size_t bytes = nd * rounded((size_t)n * 8) + (nf + ni) * rounded((size_t)n * 4);
+    CUDA_TRY(cudaMalloc(&h->tr_block, bytes));
+    char *p = static_cast<char *>(h->tr_block);
+    char *const end = p + bytes;
+    auto take = [&](size_t sz) { char *q = p; p += rounded(sz); return q; };
+    Tracers &T = h->tr;
+    T.n = n;
+    std::vector<double> d(nd * (size_t)n);
+    std::vector<float> f(nf * (size_t)n);
+    std::vector<int> iv(ni * (size_t)n);
+    for (int t = 0; t < n; ++t) {
+        const double *r = rows + 12 * (size_t)t;
+        d[0 * (size_t)n + t] = r[0]; d[1 * (size_t)n + t] = r[1];
+        d[2 * (size_t)n + t] = r[2]; d[3 * (size_t)n + t] = r[3];
+        d[4 * (size_t)n + t] = 0.0; d[5 * (size_t)n + t] = 0.0;
+        f[0 * (size_t)n + t] = (float)r[4]; f[1 * (size_t)n + t] = (float)r[5];
+        for (int q = 0; q < 6; ++q) iv[q * (size_t)n + t] = (int)r[6 + q];
+        iv[6 * (size_t)n + t] = 1;
+    }
+    double **dp[6] = {&T.x, &T.y, &T.vx, &T.vy, &T.rec_pre, &T.rec_tem};
+    for (int q = 0; q < 6; ++q) {
+        *dp[q] = reinterpret_cast<double *>(take((size_t)n * 8));
+        CUDA_TRY(cudaMemcpy(*dp[q], d.data() + q * (size_t)n, (size_t)n * 8, cudaMemcpyHostToDevice));
+    }
+    float **fp[2] = {&T.mpre, &T.mtem};
+    for (int q = 0; q < 2; ++q) {
+        *fp[q] = reinterpret_cast<float *>(take((size_t)n * 4));
+        CUDA_TRY(cudaMemcpy(*fp[q], f.data() + q * (size_t)n, (size_t)n * 4, cudaMemcpyHostToDevice));
+    }
+    int **ip[7] = {&T.gx, &T.gy, &T.tag, &T.matid, &T.cx, &T.cy, &T.alive};
+    for (int q = 0; q < 7; ++q) {
+        *ip[q] = reinterpret_cast<int *>(take((size_t)n * 4));
+        CUDA_TRY(cudaMemcpy(*ip[q], iv.data() + q * (size_t)n, (size_t)n * 4, cudaMemcpyHostToDevice));
+    }
+    if (p > end) return fail(SALEC_ERR_STATE, "tracer block layout overflow");
     return SALEC_OK;
 }
 
 int salec_gpu_get_tracers(salec_gpu *h, double *rows, int *n)
 {
-    (void)rows;
     if (!h || !n) return fail(SALEC_ERR_ARG, "bad argument");
-    *n = 0;
+    const Tracers &T = h->tr;
+    const size_t m = (size_t)T.n;
+    std::vector<double> d(6 * m);
+    std::vector<float> f(2 * m);
+    std::vector<int> iv(7 * m);
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (m) {
+        const double *dp[6] = {T.x, T.y, T.vx, T.vy, T.rec_pre, T.rec_tem};
+        for (int q = 0; q < 6; ++q) CUDA_TRY(cudaMemcpy(d.data() + q * m, dp[q], m * 8, cudaMemcpyDeviceToHost));
+        const float *fp[2] = {T.mpre, T.mtem};
+        for (int q = 0; q < 2; ++q) CUDA_TRY(cudaMemcpy(f.data() + q * m, fp[q], m * 4, cudaMemcpyDeviceToHost));
+        const int *ip[7] = {T.gx, T.gy, T.tag, T.matid, T.cx, T.cy, T.alive};
+        for (int q = 0; q < 7; ++q) CUDA_TRY(cudaMemcpy(iv.data() + q * m, ip[q], m * 4, cudaMemcpyDeviceToHost));
+    }
+    int live = 0;
+    for (size_t t = 0; t < m; ++t)
+        if (iv[6 * m + t]) ++live;
+    if (!rows) { *n = live; return SALEC_OK; }
+    if (*n < live) { int cap = *n; *n = live; return fail(SALEC_ERR_ARG, "tracer buffer holds " + std::to_string(cap) + " rows, need " + std::to_string(live)); }
+    int o = 0;
+    for (size_t t = 0; t < m; ++t) {
+        if (!iv[6 * m + t]) continue;
+        double *r = rows + 12 * (size_t)o++;
+        r[0] = d[0 * m + t]; r[1] = d[1 * m + t]; r[2] = d[2 * m + t]; r[3] = d[3 * m + t];
+        r[4] = f[0 * m + t]; r[5] = f[1 * m + t];
+        for (int q = 0; q < 6; ++q) r[6 + q] = iv[q * m + t];
+    }
+    *n = live;
     return SALEC_OK;
 }
 

@@ -644,6 +644,83 @@ __global__ void k_energy(const Ctx c)
     c.f.e_cvs[p] = wind(c.f.e_cvs[p] + dcvs * dt, -10.0, 10.0);
 }
 
+// ============================================================ phase 11: tracers
+// fl_update_node (src/tracer.c:52-175): bilinear interpolation of the vertex displacement
+// (or, in cells with vacuum, ballistic motion under the interpolated vertex acceleration),
+// ejecta tagging, peak pressure/temperature, and the cell index walk; a tracer that leaves
+// the interior cells is deleted.
+__device__ __forceinline__ double bilinear4(const double *v, double xi, double eta)
+{
+    // shape functions of the reference's IpB order: lb, rb, ru, lu (src/geometry/interpolate_fn.c:249)
+    double r = 0;
+    r += 0.25 * (1 - xi) * (1 - eta) * v[0];
+    r += 0.25 * (1 + xi) * (1 - eta) * v[1];
+    r += 0.25 * (1 + xi) * (1 + eta) * v[2];
+    r += 0.25 * (1 - xi) * (1 + eta) * v[3];
+    return r;
+}
+
+__global__ void k_tracers(const Ctx c)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const Tracers &T = c.tr;
+    if (t >= T.n || !T.alive[t]) return;
+    const int k = T.cx[t], j = T.cy[t];
+    const double dt = c.scal->dt;
+    const long long vl[4] = {KIDX(k, j), KIDX(k + 1, j), KIDX(k + 1, j + 1), KIDX(k, j + 1)};
+    // vertex coordinate lines of the reference's tracer list (v_pos along row 1 and column 1)
+    const double vxk = c.f.v_pos[KIDX(k, 1)], vxk1 = c.f.v_pos[KIDX(k + 1, 1)];
+    const double vyj = PLN(c.f.v_pos, 1)[KIDX(1, j)], vyj1 = PLN(c.f.v_pos, 1)[KIDX(1, j + 1)];
+    double px = T.x[t], py = T.y[t];
+    double rx = 1.0 * px + -1.0 * c.f.v_pos[vl[0]];
+    double ry = 1.0 * py + -1.0 * PLN(c.f.v_pos, 1)[vl[0]];
+    rx = rx / (vxk1 - vxk) * 2.0 - 1.0;
+    ry = ry / (vyj1 - vyj) * 2.0 - 1.0;
+    double q[4];
+    if (c.f.m_vof[KIDX(k, j)] > SALEC_TOLVOF) {
+        for (int a = 0; a < 4; ++a) q[a] = c.f.v_acc[vl[a]];
+        const double bx = bilinear4(q, rx, ry);
+        for (int a = 0; a < 4; ++a) q[a] = PLN(c.f.v_acc, 1)[vl[a]];
+        const double by = bilinear4(q, rx, ry);
+        const double hdt2 = 0.5 * dt * dt;
+        const double dx = dt * T.vx[t] + hdt2 * bx;
+        const double dy = dt * T.vy[t] + hdt2 * by;
+        T.vx[t] += dt * bx;
+        T.vy[t] += dt * by;
+        px += 1.0 * dx;
+        py += 1.0 * dy;
+    } else {
+        for (int a = 0; a < 4; ++a) q[a] = c.f.v_dis[vl[a]];
+        const double dx = bilinear4(q, rx, ry);
+        for (int a = 0; a < 4; ++a) q[a] = PLN(c.f.v_dis, 1)[vl[a]];
+        const double dy = bilinear4(q, rx, ry);
+        for (int a = 0; a < 4; ++a) q[a] = c.f.v_vel[vl[a]];
+        const double ux = bilinear4(q, rx, ry);
+        for (int a = 0; a < 4; ++a) q[a] = PLN(c.f.v_vel, 1)[vl[a]];
+        const double uy = bilinear4(q, rx, ry);
+        px += 1.0 * dx;
+        py += 1.0 * dy;
+        T.vx[t] = 1.0 * ux;
+        T.vy[t] = 1.0 * uy;
+    }
+    T.x[t] = px;
+    T.y[t] = py;
+    if (T.matid[t] > 0 && py > c.rp.threshold_z) T.matid[t] = -T.matid[t];
+    const long long e = KIDX(k, j);
+    const double pre = c.f.e_pre[e], tem = c.f.e_tem[e];
+    T.mpre[t] = (float)((double)T.mpre[t] > pre ? (double)T.mpre[t] : pre);
+    T.mtem[t] = (float)((double)T.mtem[t] > tem ? (double)T.mtem[t] : tem);
+    T.rec_pre[t] = pre;
+    T.rec_tem[t] = tem;
+    // GET_OFFSET2 walk of the cell index, then the interior test of fl_node_nei
+    const int ox = px < vxk ? -1 : ((px < vxk1 && px >= vxk) ? 0 : 1);
+    const int oy = py < vyj ? -1 : ((py < vyj1 && py >= vyj) ? 0 : 1);
+    const int nk = k + ox, nj = j + oy;
+    T.cx[t] = nk;
+    T.cy[t] = nj;
+    if (!(nk >= 2 && nk <= c.d.enx - 3 && nj >= 2 && nj <= c.d.eny - 3)) T.alive[t] = 0;
+}
+
 // ============================================================ phase 12: face flux volumes
 // calculate_flux_mixed (src/advect.c:861-1136) with _calculate_flux_set_bphi (:1138-1223):
 // swept face volumes, geometric cut-line reconstruction of the primary material, algebraic

@@ -86,6 +86,8 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_get_tracers": ([vp, P_D, ctypes.POINTER(c_i)], c_i),
             "salec_gpu_check": ([vp, ctypes.POINTER(c_ll)], c_i),
             "salec_gpu_func_index": ([ctypes.c_char_p], c_i),
+            "salec_boundary_map": ([c_i, c_i, c_i, c_i, c_i, ctypes.POINTER(c_i), ctypes.POINTER(c_i),
+                                    ctypes.POINTER(c_i), ctypes.POINTER(c_i), ctypes.POINTER(ctypes.c_uint)], c_i),
             "salec_gpu_last_error": ([], ctypes.c_char_p),
         }
         for name, (args, res) in sig.items():
@@ -120,6 +122,36 @@ def field_index(name: str) -> int:
     if k < 0:
         raise KeyError(name)
     return k
+
+
+def boundary_map(kind: int, pattern: int, nx: int, ny: int, ncomp: int, go: Sequence[int]):
+    """Gather map of a ghost (kind 0) or restriction (kind 1) table: arrays dst, src, ops."""
+    g = (c_i * 4)(*go)
+    n = c_i(0)
+    _check(lib().salec_boundary_map(kind, pattern, nx, ny, ncomp, g, ctypes.byref(n), None, None, None),
+           "boundary_map")
+    dst = np.zeros(max(n.value, 1), np.int32)
+    src = np.zeros(max(n.value, 1), np.int32)
+    ops = np.zeros(max(n.value, 1), np.uint32)
+    ip = ctypes.POINTER(c_i)
+    _check(lib().salec_boundary_map(kind, pattern, nx, ny, ncomp, g, ctypes.byref(n), dst.ctypes.data_as(ip),
+                                    src.ctypes.data_as(ip), ops.ctypes.data_as(ctypes.POINTER(ctypes.c_uint))),
+           "boundary_map")
+    return dst[: n.value], src[: n.value], ops[: n.value]
+
+
+def apply_boundary_map(field: np.ndarray, dst, src, ops) -> np.ndarray:
+    """Apply a gather map to a (ny, nx, ncomp) array on the host (numpy restatement of k_gather)."""
+    f = field.reshape(-1, field.shape[-1])
+    out = f.copy()
+    nc = f.shape[1]
+    for c in range(nc):
+        op = (ops >> (3 * c)) & 7
+        v = f[src, c]
+        r = np.where(op == 0, v, np.where(op == 1, -1.0 * v, np.where(op == 2, np.abs(v),
+                     np.where(op == 3, -np.abs(v), np.where(op == 4, 0.0, -0.0)))))
+        out[dst, c] = r
+    return out.reshape(field.shape)
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -211,8 +243,9 @@ class Simulation:
         r = np.ascontiguousarray(rows, dtype=np.float64).reshape(-1, 12)
         _check(lib().salec_gpu_set_tracers(self.h, r.shape[0], _ptr(r)), "set_tracers")
 
-    def get_tracers(self, capacity: int) -> np.ndarray:
-        out = np.zeros((max(capacity, 1), 12))
-        n = c_i(capacity)
+    def get_tracers(self) -> np.ndarray:
+        n = c_i(0)
+        _check(lib().salec_gpu_get_tracers(self.h, None, ctypes.byref(n)), "count tracers")
+        out = np.zeros((max(n.value, 1), 12))
         _check(lib().salec_gpu_get_tracers(self.h, _ptr(out), ctypes.byref(n)), "get_tracers")
         return out[: n.value]

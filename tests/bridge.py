@@ -92,6 +92,7 @@ def gpu_from_oracle() -> capi.Simulation:
     sim = capi.Simulation(run, materials_from_oracle(run.nmat))
     for name in UPLOAD_FIELDS:
         sim.set_field(name, ref.get(name))
+    sim.set_tracers(ref.tracers())
     return sim
 
 

@@ -1,0 +1,77 @@
+"""Oracle trajectories for the GPU parity tests (test infrastructure).
+
+``oracle_trajectory`` runs in a fresh spawned process (the reference keeps global state):
+it writes a small synthetic deck, runs the reference's own initialisation, and records
+the initial upload set plus the evolved fields after every step. The parent process then
+drives the GPU library from the same initial state and compares.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import multiprocessing as mp
+import os
+from typing import Dict, List
+
+import numpy as np
+
+import bridge
+from bridge import ref
+
+RUN_FIELDS = [n for n, _ in bridge.capi.RunDesc._fields_]
+
+
+def oracle_trajectory(kind: str, nsteps: int, folder: str, phase_steps: int = 0) -> Dict:
+    deck, folder = bridge.write_small_deck(kind, folder)
+    ref.init(deck, folder, os.path.join(folder, "run"))
+    run = bridge.run_desc_from_oracle()
+    out = {
+        "kind": kind,
+        "run": {n: (list(getattr(run, n)) if n == "go" else getattr(run, n)) for n in RUN_FIELDS},
+        "mats": bridge.materials_from_oracle(run.nmat),
+        "init": {n: ref.get(n) for n in bridge.UPLOAD_FIELDS},
+        "tracers0": ref.tracers(),
+        "phases": [],
+        "steps": [],
+    }
+    # optional phase-by-phase record of the first steps
+    for s in range(phase_steps):
+        for p in range(16):
+            ref.phase(p)
+            out["phases"].append({n: ref.get(n) for n in bridge.STATE_FIELDS})
+    for s in range(phase_steps, nsteps):
+        ref.step()
+        rec = {n: ref.get(n) for n in bridge.STATE_FIELDS}
+        rec["dt"] = ref.scalar("dt")
+        rec["time"] = ref.scalar("time")
+        rec["tracers"] = ref.tracers()
+        out["steps"].append(rec)
+    return out
+
+
+def trajectories(kinds: List[str], nsteps: int, root: str, phase_steps: int = 0) -> Dict[str, Dict]:
+    """Run several oracle trajectories in parallel spawned processes."""
+    ctx = mp.get_context("spawn")
+    workers = max(1, min(len(kinds), os.cpu_count() or 1))
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=ctx) as ex:
+        futs = {k: ex.submit(oracle_trajectory, k, nsteps, os.path.join(root, k), phase_steps) for k in kinds}
+        return {k: f.result() for k, f in futs.items()}
+
+
+def simulation_from_record(rec: Dict):
+    run = bridge.capi.RunDesc()
+    for n, v in rec["run"].items():
+        if n == "go":
+            for k in range(4):
+                run.go[k] = int(v[k])
+        else:
+            setattr(run, n, v)
+    sim = bridge.capi.Simulation(run, rec["mats"])
+    for n, a in rec["init"].items():
+        sim.set_field(n, a)
+    sim.set_tracers(rec["tracers0"])
+    return sim
+
+
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
