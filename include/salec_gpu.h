@@ -111,6 +111,18 @@ typedef struct salec_material_desc {
 int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats, salec_gpu **out);
 int salec_gpu_destroy(salec_gpu *h);
 
+/*
+ * Create a handle directly from a reference input deck (.inp) and the folder holding its EOS
+ * files (the reference's `salec2d deck.inp eos_dir`), without the reference's host code: the
+ * start-up of src/salec2d.c:45-105 (deck, materials, EOS tables, geometry, hydrostatic target
+ * profile, material distribution, first EOS call, damping reference state, vertex velocities,
+ * tracers) is restated by the library. A deck for an npgx x npgy process grid is run as one
+ * domain of (npgx*npx) x (npgy*npy) cells.
+ */
+int salec_gpu_create_from_deck(const char *deck_path, const char *eos_dir, salec_gpu **out);
+/* The run description of a handle (for a deck-created handle: the values derived from the deck). */
+int salec_gpu_get_run(const salec_gpu *h, salec_run_desc *out);
+
 /* Field names are the reference's member names of sale2d_var (e.g. "m_vof", "v_vel",
  * "bx_phi", "y_profile"). Returns the field index or -1. */
 int salec_gpu_field_index(const char *name);
@@ -122,10 +134,23 @@ int salec_gpu_get_field(salec_gpu *h, int field, double *host, long long n);
 
 /* Advance nsteps full cycles: the loop body of src/salec2d.c:115-272 without the output point. */
 int salec_gpu_step(salec_gpu *h, int nsteps);
-/* Run phases first..last of one cycle (numbering of oracle/ref_driver.c); for stepwise checks. */
+/* Run phases first..last of one cycle, for stepwise checks and timing. Phases follow the
+ * reference's loop body (src/salec2d.c): 0 surface profile, 1 vertex volume fractions,
+ * 2 vertex momentum + restriction, 3 cell velocity + ghosts, 4 void vertices, 5 velocity
+ * gradient, viscosity and CFL candidates, 6 time step, 7 vibration/stress/damage, 8 vertex
+ * acceleration (+ ghosts, restriction), 9 vertex displacement + restriction, 10 internal
+ * energy, 11 tracers, 12 face fluxes (+ ghosts), 13 strength condition, 14 remap, damping,
+ * ejecta drag and EOS, 15 cycle control. */
 int salec_gpu_phases(salec_gpu *h, int first, int last);
 /* Block until the handle's stream is idle. */
 int salec_gpu_sync(salec_gpu *h);
+/* The CUDA stream (cudaStream_t) all work of the handle is queued on. */
+int salec_gpu_stream(salec_gpu *h, void **stream);
+/* Per-phase device timing: when enabled, every phase run is bracketed by CUDA events on the
+ * handle's stream; salec_gpu_phase_times() waits for the stream and returns, per phase 0..15,
+ * the summed milliseconds and the number of runs since the last call (or since enabling). */
+int salec_gpu_profile(salec_gpu *h, int enable);
+int salec_gpu_phase_times(salec_gpu *h, double *ms, long long *count);
 
 /* Scalars: "dt", "time", "i_step", "damp_time", "max_dt". */
 int salec_gpu_get_scalar(salec_gpu *h, const char *name, double *value);

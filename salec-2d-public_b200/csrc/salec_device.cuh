@@ -73,6 +73,7 @@ struct Scal {
     unsigned long long dt_acc;    // ordered-bits MIN accumulator of the CFL candidates
     long long i_step;
     unsigned long long nan_count; // used by salec_gpu_check
+    unsigned long long aux;       // ordered-bits MAX accumulator used at initialisation
 };
 
 struct Fields {
@@ -107,13 +108,13 @@ struct Ctx {
 };
 
 // ------------------------------------------------------------------ small helpers
-__device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }   // MIN / Min
-__device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }   // MAX / Max
-__device__ __forceinline__ double wind(double x, double lo, double hi)
+__host__ __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }   // MIN / Min
+__host__ __device__ __forceinline__ double dmax(double a, double b) { return a > b ? a : b; }   // MAX / Max
+__host__ __device__ __forceinline__ double wind(double x, double lo, double hi)
 {
     return x < lo ? lo : (x > hi ? hi : x);
 }
-__device__ __forceinline__ double sqrt_trunc(double x) { return x < 1.0e-2 ? -sqrt(fabs(x)) : sqrt(x); }
+__host__ __device__ __forceinline__ double sqrt_trunc(double x) { return x < 1.0e-2 ? -sqrt(fabs(x)) : sqrt(x); }
 
 // Order-preserving map of doubles to unsigned integers (for atomic MIN of doubles).
 __host__ __device__ __forceinline__ unsigned long long ord_encode(double v)
@@ -160,7 +161,7 @@ __device__ __forceinline__ int bisearch(double x, const double *xs, int n)
 // ------------------------------------------------------------------ Tillotson EOS
 // Tillotson (1962) as evaluated in src/eos/eos_state.c:322-438 (TillCold, TillHot, TillTran,
 // TillPres); t = {rho0, Cv, A, B, E0, a, b, alpha, beta, Eiv, Ecv, Tref, StepDen}.
-__device__ __forceinline__ void till_pressure(const double *t, double E, double rho, double &pres, double &cs)
+__host__ __device__ __forceinline__ void till_pressure(const double *t, double E, double rho, double &pres, double &cs)
 {
     const double rho0 = t[0], A = t[2], B = t[3], E0 = t[4], a = t[5], b = t[6];
     const double al = t[7], be = t[8], Eiv = t[9], Ecv = t[10];

@@ -60,6 +60,8 @@ __global__ void k_tracers(const Ctx c);
 __global__ void k_flux(const Ctx c, int pass);
 __global__ void k_remap_damp_state(const Ctx c, int do_remap, int do_damp, int do_ejecta, int do_state);
 __global__ void k_cycle(const Ctx c);
+__global__ void k_record_reference_state(const Ctx c);
+__global__ void k_init_vertex_velocity(const Ctx c);
 __global__ void k_gather(GatherBatch g, int mode, double *scratch);
 __global__ void k_aos_to_planes(const double *aos, double *base, long long plane, int P, int nx, int ny, int nc);
 __global__ void k_planes_to_aos(const double *base, double *aos, long long plane, int P, int nx, int ny, int nc);

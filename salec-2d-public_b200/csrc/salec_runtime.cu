@@ -110,9 +110,15 @@ struct salec_gpu {
     size_t scratch_doubles = 0;
     double *staging = nullptr;   // AoS staging for field transfer
     size_t staging_doubles = 0;
-    Gather g_mvof, g_dvel_den, g_evel, g_pre_ste_q, g_flux_state, r_vel, r_acc, r_dis;
+    Gather g_mvof, g_dvel_den, g_evel, g_pre_ste_q, g_flux_state, r_vel, r_acc, r_dis, g_init;
     Tracers tr{};
     void *tr_block = nullptr;   // one allocation holding every tracer array
+    salec_run_desc run{};       // the description the handle was created from
+    // optional per-phase timing with CUDA events on the handle's stream
+    int profiling = 0;
+    std::vector<cudaEvent_t> ev_a, ev_b;
+    std::vector<int> ev_phase;
+    size_t ev_used = 0;
 
     Ctx ctx() const
     {
@@ -300,6 +306,10 @@ int build_gathers(salec_gpu *h)
         fs.push_back(gm("e_cvs", GP_ALWAYS_COPY));
     }
     if ((rc = make_gather(h, h->g_flux_state, fs))) return rc;
+    if ((rc = make_gather(h, h->g_init,
+                          {gm("e_den", GP_DENSITY), gm("e_pre", GP_ALWAYS_COPY), gm("e_ste", GP_STRESS),
+                           gm("m_eng", GP_DENSITY), gm("m_pty", GP_ALWAYS_COPY), gm("e_cvs", GP_ALWAYS_COPY)})))
+        return rc;
     if ((rc = make_gather(h, h->r_vel, {rm("v_vel")}))) return rc;
     if ((rc = make_gather(h, h->r_acc, {rm("v_acc")}))) return rc;
     if ((rc = make_gather(h, h->r_dis, {rm("v_dis")}))) return rc;
@@ -392,11 +402,46 @@ void release(salec_gpu *h)
     if (h->scal_host) cudaFreeHost(h->scal_host);
     if (h->mat) cudaFree(h->mat);
     if (h->tr_block) cudaFree(h->tr_block);
+    for (auto e : h->ev_a) cudaEventDestroy(e);
+    for (auto e : h->ev_b) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
 
 } // namespace
+
+// Last start-up steps on the device (src/salec2d.c:76-94): first EOS call, ghost fills,
+// damping reference state and arrival time, vertex velocities, cleared cell velocities.
+int salec_internal_finish_init(salec_gpu *h, double damp_time_in, double *damp_time_out)
+{
+    const Ctx c = h->ctx();
+    const dim3 blk(32, 8);
+    const dim3 gc = grid2(h->d.enx, h->d.eny, blk), gv = grid2(h->d.vnx, h->d.vny, blk);
+    k_remap_damp_state<<<gc, blk, 0, h->stream>>>(c, 0, 0, 0, 1);
+    int rc = run_gather(h, h->g_init);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemsetAsync(&h->scal->aux, 0, sizeof(unsigned long long), h->stream));
+    k_record_reference_state<<<gc, blk, 0, h->stream>>>(c);
+    CUDA_TRY(cudaGetLastError());
+    unsigned long long mx = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h->scal_host->aux, &h->scal->aux, sizeof(mx), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    mx = h->scal_host->aux;
+    const double local = mx ? ord_decode(mx) : 0.0;
+    const double dt2 = local * 2.0;
+    h->rp.damp_time = dmax(dt2, damp_time_in);
+    if (damp_time_out) *damp_time_out = h->rp.damp_time;
+    k_init_vertex_velocity<<<gv, blk, 0, h->stream>>>(h->ctx());
+    CUDA_TRY(cudaGetLastError());
+    for (const char *nm : {"e_vel", "e_ste", "e_dvel"}) {
+        int fid = field_by_name(nm);
+        CUDA_TRY(cudaMemsetAsync(field_ptr(h, fid), 0, (size_t)field_ncomp(h, fid) * h->d.PL * sizeof(double), h->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return SALEC_OK;
+}
+
+int salec_internal_fail(int code, const char *msg) { return fail(code, msg ? msg : "error"); }
 
 // ================================================================== C ABI
 extern "C" {
@@ -434,6 +479,14 @@ int salec_boundary_map(int kind, int pattern, int nx, int ny, int ncomp, const i
     return SALEC_OK;
 }
 
+int salec_gpu_get_run(const salec_gpu *h, salec_run_desc *out)
+{
+    if (!h || !out) return fail(SALEC_ERR_ARG, "null argument");
+    *out = h->run;
+    out->damp_time = h->rp.damp_time;
+    return SALEC_OK;
+}
+
 int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats, salec_gpu **out)
 {
     if (!run || !mats || !out) return fail(SALEC_ERR_ARG, "null argument");
@@ -457,6 +510,7 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
     d.R = d.vny;
     d.PL = (((long long)d.P * d.R + 31) / 32) * 32;
     for (int k = 0; k < 4; ++k) h->go[k] = run->go[k];
+    h->run = *run;
     RunParams &rp = h->rp;
     rp.damp_type = run->damp_type; rp.partpres = run->partpres; rp.porosity_model = run->porosity_model;
     rp.acoustic_fluid = run->acoustic_fluid; rp.tensile_failure = run->tensile_failure;
@@ -551,8 +605,25 @@ int salec_gpu_phases(salec_gpu *h, int first, int last)
     if (!h) return fail(SALEC_ERR_ARG, "null handle");
     if (first < 0 || last > 15 || first > last) return fail(SALEC_ERR_ARG, "phase range must lie in [0, 15]");
     for (int p = first; p <= last; ++p) {
-        int rc = run_phase(h, p);
-        if (rc) return rc;
+        if (h->profiling) {
+            if (h->ev_used == h->ev_a.size()) {
+                cudaEvent_t a, b;
+                CUDA_TRY(cudaEventCreate(&a));
+                CUDA_TRY(cudaEventCreate(&b));
+                h->ev_a.push_back(a);
+                h->ev_b.push_back(b);
+                h->ev_phase.push_back(0);
+            }
+            const size_t k = h->ev_used++;
+            h->ev_phase[k] = p;
+            CUDA_TRY(cudaEventRecord(h->ev_a[k], h->stream));
+            int rc = run_phase(h, p);
+            if (rc) return rc;
+            CUDA_TRY(cudaEventRecord(h->ev_b[k], h->stream));
+        } else {
+            int rc = run_phase(h, p);
+            if (rc) return rc;
+        }
     }
     return SALEC_OK;
 }
@@ -565,6 +636,36 @@ int salec_gpu_step(salec_gpu *h, int nsteps)
         int rc = salec_gpu_phases(h, 0, 15);
         if (rc) return rc;
     }
+    return SALEC_OK;
+}
+
+int salec_gpu_stream(salec_gpu *h, void **stream)
+{
+    if (!h || !stream) return fail(SALEC_ERR_ARG, "null argument");
+    *stream = (void *)h->stream;
+    return SALEC_OK;
+}
+
+int salec_gpu_profile(salec_gpu *h, int enable)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    h->profiling = enable ? 1 : 0;
+    h->ev_used = 0;
+    return SALEC_OK;
+}
+
+int salec_gpu_phase_times(salec_gpu *h, double *ms, long long *count)
+{
+    if (!h || !ms || !count) return fail(SALEC_ERR_ARG, "null argument");
+    for (int p = 0; p < 16; ++p) { ms[p] = 0.0; count[p] = 0; }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (size_t k = 0; k < h->ev_used; ++k) {
+        float t = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&t, h->ev_a[k], h->ev_b[k]));
+        ms[h->ev_phase[k]] += t;
+        count[h->ev_phase[k]] += 1;
+    }
+    h->ev_used = 0;
     return SALEC_OK;
 }
 

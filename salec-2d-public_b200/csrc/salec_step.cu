@@ -1310,6 +1310,62 @@ __global__ void k_cycle(const Ctx c)
     }
 }
 
+// ============================================================ initialisation sweeps
+// record_avg_value (src/sale2d.c:1562-1627): reference state of the damping layers and the
+// latest arrival time of the impact wave at a damped cell (MAX over cells).
+__global__ void k_record_reference_state(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    unsigned long long cand = 0ULL;
+    if (i < c.d.enx && j < c.d.eny) {
+        const long long p = KIDX(i, j);
+        PLN(c.f.e_dampref, 0)[p] = c.f.e_den[p];
+        const double x = c.f.e_pos[p], y = PLN(c.f.e_pos, 1)[p];
+        double len = 0.;
+        len += x * x;
+        len += y * y;
+        len = sqrt(len);
+        const double csd = c.f.e_csd[p];
+        if ((c.f.e_sigma[p] > 0. || PLN(c.f.e_sigma, 1)[p] > 0.) && csd > 2.0) cand = ord_encode(len / csd);
+        double s = 0.0;
+        for (int m = 1; m < c.d.nmat; ++m) s += PLN(c.f.m_vof, m)[p] * PLN(c.f.m_eng, m)[p];
+        PLN(c.f.e_dampref, 1)[p] = s;
+        PLN(c.f.e_dampref, 2)[p] = c.f.e_pre[p];
+    }
+    for (int o = 16; o > 0; o >>= 1) cand = max(cand, __shfl_xor_sync(0xffffffffu, cand, o));
+    if (((threadIdx.y * blockDim.x + threadIdx.x) & 31) == 0 && cand) atomicMax(&c.scal->aux, cand);
+}
+
+// init_v_field (src/sale2d.c:1897-1957): vertex velocity and mass from the cell velocities.
+__global__ void k_init_vertex_velocity(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!vert_active(c, i, j)) return;
+    const long long p = KIDX(i, j);
+    const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
+    double vx = 0., vy = 0., em = 0., ev = 0.;
+    for (int k = 0; k < 4; ++k) {
+        const double lv = PLN(c.f.v_vol, k + 1)[p];
+        const double w = c.f.e_den[cl[k]] * lv;
+        vx += w * c.f.e_vel[cl[k]];
+        vy += w * PLN(c.f.e_vel, 1)[cl[k]];
+        em += c.f.e_den[cl[k]] * lv;
+        ev += lv;
+    }
+    if (em > SALEC_TOLRHO * ev) {
+        const double s = 1.0 / em;
+        vx *= s; vy *= s;
+        c.f.v_mass[p] = em;
+        PLN(c.f.v_mass, 1)[p] = ev;
+    } else {
+        vx = vy = 0.;
+        c.f.v_mass[p] = 0.;
+        PLN(c.f.v_mass, 1)[p] = 0.;
+    }
+    c.f.v_vel[p] = vx;
+    PLN(c.f.v_vel, 1)[p] = vy;
+}
+
 // ============================================================ boundary gathers
 // Apply a precomputed gather map (built on the host from the reference's ghost and
 // restriction tables): dst[k] = op_c(src[k]) per component c. In-place when no source is also

@@ -86,6 +86,11 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_get_tracers": ([vp, P_D, ctypes.POINTER(c_i)], c_i),
             "salec_gpu_check": ([vp, ctypes.POINTER(c_ll)], c_i),
             "salec_gpu_func_index": ([ctypes.c_char_p], c_i),
+            "salec_gpu_create_from_deck": ([ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(vp)], c_i),
+            "salec_gpu_get_run": ([vp, ctypes.POINTER(RunDesc)], c_i),
+            "salec_gpu_stream": ([vp, ctypes.POINTER(vp)], c_i),
+            "salec_gpu_profile": ([vp, c_i], c_i),
+            "salec_gpu_phase_times": ([vp, P_D, ctypes.POINTER(c_ll)], c_i),
             "salec_boundary_map": ([c_i, c_i, c_i, c_i, c_i, ctypes.POINTER(c_i), ctypes.POINTER(c_i),
                                     ctypes.POINTER(c_i), ctypes.POINTER(c_i), ctypes.POINTER(ctypes.c_uint)], c_i),
             "salec_gpu_last_error": ([], ctypes.c_char_p),
@@ -160,6 +165,37 @@ def _ptr(a: Optional[np.ndarray]):
 
 class Simulation:
     """One device-resident simulation (a salec_gpu handle)."""
+
+    @classmethod
+    def from_deck(cls, deck: str, eos_dir: str) -> "Simulation":
+        """Create a simulation from a reference input deck and its EOS folder (no reference code)."""
+        self = cls.__new__(cls)
+        self._keep = []
+        h = ctypes.c_void_p()
+        _check(lib().salec_gpu_create_from_deck(deck.encode(), eos_dir.encode(), ctypes.byref(h)),
+               "salec_gpu_create_from_deck")
+        self.h = h
+        self.run = self.get_run()
+        return self
+
+    def get_run(self) -> RunDesc:
+        r = RunDesc()
+        _check(lib().salec_gpu_get_run(self.h, ctypes.byref(r)), "get_run")
+        return r
+
+    def stream(self) -> int:
+        p = ctypes.c_void_p()
+        _check(lib().salec_gpu_stream(self.h, ctypes.byref(p)), "stream")
+        return int(p.value or 0)
+
+    def profile(self, enable: bool) -> None:
+        _check(lib().salec_gpu_profile(self.h, 1 if enable else 0), "profile")
+
+    def phase_times(self):
+        ms = (c_d * 16)()
+        cnt = (c_ll * 16)()
+        _check(lib().salec_gpu_phase_times(self.h, ms, cnt), "phase_times")
+        return list(ms), list(cnt)
 
     def __init__(self, run: RunDesc, materials: Sequence[Dict]):
         """``materials``: one dict per material index (entry 0, vacuum, may be empty) with the

@@ -67,3 +67,45 @@ def test_step_parity(records, cuda_device, kind):
         assert tj.rel_l2(tg[:, 4:6], tr[:, 4:6]) <= 1e-6   # peak P/T are float32 in the reference
     assert sim.check() == 0
     sim.close()
+
+
+INIT_KINDS = ["base", "two_mat", "sieden_projectile", "porous", "sbc_tensile"]
+# fields computed by the host initialiser with the reference's own arithmetic: bit-exact
+INIT_EXACT = ["v_pos", "e_pos", "e_vol", "e_grad", "v_vol", "v_subvol", "v_suf", "e_sigma", "bx_normal",
+              "by_normal", "v_bf", "m_vof", "m_pty", "e_wpt", "e_tem", "e_dam"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", INIT_KINDS)
+def test_deck_initialiser_matches_reference_init(records, cuda_device, tmp_path, kind):
+    """salec_gpu_create_from_deck (no reference code) against the reference's start-up."""
+    from salec_b200 import capi
+    rec = records[kind]
+    deck, folder = bridge.write_small_deck(kind, str(tmp_path))
+    sim = capi.Simulation.from_deck(deck, folder)
+    run = sim.get_run()
+    for name, v in rec["run"].items():
+        if name == "go":
+            assert list(run.go) == list(v)
+        elif name not in ("dt", "time", "i_step"):
+            assert getattr(run, name) == pytest.approx(v, rel=1e-12, abs=0.0), name
+    for name in bridge.UPLOAD_FIELDS:
+        got, want = sim.get_field(name), rec["init"][name]
+        if name in INIT_EXACT:
+            assert np.array_equal(got, want), "%s differs from the reference init" % name
+        elif name == "v_laplace":
+            # only evaluated inside the ANC taper band; zero (possibly -0.0) elsewhere in the reference
+            assert np.array_equal(got == 0, want == 0) and tj.rel_l2(got, want) == 0.0, name
+        else:
+            assert tj.rel_l2(got, want) <= 1e-12, "%s rel-L2 %.3e" % (name, tj.rel_l2(got, want))
+    tg, tr = sim.get_tracers(), rec["tracers0"]
+    assert np.array_equal(tg[:, 6:12], tr[:, 6:12])
+    assert tj.rel_l2(tg[:, :4], tr[:, :4]) <= 1e-12
+    # the deck-initialised run then tracks the reference's own run
+    # rec["steps"][0] is the state after three steps (two were recorded phase by phase)
+    for s, want in enumerate(rec["steps"][:10], start=2):
+        sim.step(3 if s == 2 else 1)
+        for n in bridge.STATE_FIELDS:
+            err = tj.rel_l2(sim.get_field(n), want[n])
+            assert err <= TOL_L2, "%s step %d field %s rel-L2 %.3e" % (kind, s, n, err)
+    sim.close()
