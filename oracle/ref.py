@@ -50,6 +50,7 @@ def lib() -> ctypes.CDLL:
             "ref_eos_state": ([c_i, c_d, c_d, c_d, c_d, pd], c_i),
             "ref_tracer_count": ([], c_i), "ref_get_tracers": ([pd], c_i),
             "ref_ghost_fill": ([c_s], c_i), "ref_restrict": ([c_s], c_i),
+            "ref_init_adopt": ([c_d], c_i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -74,6 +75,11 @@ def init(deck: str, eosdir: str, workdir: str, material: bool = True) -> None:
     if material:
         _check(L.ref_init_material(), "init_material")
         _check(L.ref_init_finish(), "init_finish")
+
+
+def init_adopt(damp_time: float) -> None:
+    """After init(..., material=False) and set() of every field: make the adopted state steppable."""
+    _check(lib().ref_init_adopt(float(damp_time)), "init_adopt")
 
 
 def init_material() -> None:

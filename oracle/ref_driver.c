@@ -133,6 +133,24 @@ int ref_init_finish(void)
     return 0;
 }
 
+/*
+ * Adopt a complete initial state set by the caller (every field through ref_set_field after
+ * ref_init_begin) instead of running the reference's material set-up: records the damping
+ * time, builds the tracer list from the adopted fields (init_sale2d_tracer,
+ * src/sale2d.c:2081-2091) and makes the step loop available. Used to time the reference's
+ * step on exactly the state another implementation starts from.
+ */
+int ref_init_adopt(double damp_time)
+{
+    if (g_stage != 1) return -1;
+    g_sale.damp_time = damp_time;
+    g_ccl.out_vts = 1;
+    g_ccl.k_out_step = 1;
+    init_sale2d_tracer(&g_sale, &g_minfo);
+    g_stage = 3;
+    return 0;
+}
+
 int ref_init(const char *deck, const char *eosdir, const char *workdir)
 {
     int rc = ref_init_begin(deck, eosdir, workdir);

@@ -119,6 +119,7 @@ struct salec_gpu {
     std::vector<cudaEvent_t> ev_a, ev_b;
     std::vector<int> ev_phase;
     size_t ev_used = 0;
+    long long launches = 0;     // kernels launched by this handle
 
     Ctx ctx() const
     {
@@ -205,6 +206,7 @@ int run_gather(salec_gpu *h, const Gather &g)
 {
     if (g.batch.total == 0) return SALEC_OK;
     const int tb = 256, nb = (g.batch.total + tb - 1) / tb;
+    h->launches += g.two_pass ? 2 : 1;
     if (!g.two_pass) {
         k_gather<<<nb, tb, 0, h->stream>>>(g.batch, 0, nullptr);
     } else {
@@ -224,6 +226,8 @@ int run_phase(salec_gpu *h, int ph)
     const dim3 gc = grid2(h->d.enx, h->d.eny, blk), gv = grid2(h->d.vnx, h->d.vny, blk);
     cudaStream_t s = h->stream;
     int rc = SALEC_OK;
+    static const int kLaunches[16] = {3, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 2, 0, 1, 1};
+    h->launches += kLaunches[ph] + (ph == 11 && h->tr.n > 0 ? 1 : 0);
     switch (ph) {
     case 0: {
         const int nb = (h->d.enx + 255) / 256;
@@ -688,6 +692,7 @@ int salec_gpu_get_scalar(salec_gpu *h, const char *name, double *value)
     else if (!strcmp(name, "dt_candidate")) *value = ord_decode(s.dt_acc);
     else if (!strcmp(name, "damp_time")) *value = h->rp.damp_time;
     else if (!strcmp(name, "max_dt")) *value = h->rp.max_dt;
+    else if (!strcmp(name, "launches")) *value = (double)h->launches;
     else return fail(SALEC_ERR_ARG, std::string("unknown scalar ") + name);
     return SALEC_OK;
 }
