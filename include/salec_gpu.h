@@ -180,6 +180,27 @@ int salec_gpu_check(salec_gpu *h, long long *n_bad);
 int salec_boundary_map(int kind, int pattern, int nx, int ny, int ncomp, const int go[4], int *n, int *dst,
                        int *src, unsigned *ops);
 
+/*
+ * CFL time step of one cycle without allocating device memory. No counterpart in the
+ * reference: it computes what calculate_dt (src/sale2d.c:1959-2016) and the Min with max_dt
+ * (src/salec2d.c:167) give, for callers that cannot call cudaMalloc while they run their time
+ * loop - a host code whose device memory belongs to its own pool allocator, or one that must
+ * not take cudaMalloc's device-wide synchronisation inside a cycle.
+ * Inputs are device planes of (nx+4) x (ny+4) doubles in the reference's cell order (x
+ * fastest, two-cell pad): cell velocity r and z, sound speed, cell scales r and z (e_pos
+ * components 2 and 3) and the vacuum volume fraction; dt_out is one device double; stream is
+ * a cudaStream_t (NULL: the default stream); the work is enqueued, not waited for.
+ * Scratch: a fixed 64 KiB array in the library's device image, held on every device that loads
+ * the library until the process exits; it limits a call to 8192 * 4096 = 33554432 interior
+ * cells (larger meshes return SALEC_ERR_ARG). The first call on a device looks the array up
+ * with that device current and should come before any stream capture. All calls share the
+ * array, so calls that overlap on the GPU race and must be ordered by the caller; each call
+ * rewrites every entry it reads, so nothing needs clearing between calls.
+ */
+int salec_cfl_dt_noalloc(int nx, int ny, const double *vel_r, const double *vel_z, const double *csd,
+                         const double *scale_r, const double *scale_z, const double *vof_vacuum,
+                         double dt_prev, double max_dt, double *dt_out, void *stream);
+
 /* Strength/damage/porosity function index for a reference name (case-insensitive), or -1. */
 int salec_gpu_func_index(const char *name);
 /* Message of the last error on this thread. */

@@ -15,7 +15,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)               # salec-2d-public_b200/
 CSRC = os.path.join(ROOT, "csrc")
 LIB = os.path.join(PKG, "libsalec_b200.so")
-SOURCES = ["salec_step.cu", "salec_runtime.cu", "salec_init.cu", "salec_ghost.cpp"]
+SOURCES = ["salec_step.cu", "salec_runtime.cu", "salec_init.cu", "salec_noalloc.cu", "salec_ghost.cpp"]
 HEADERS = ["salec_device.cuh", "salec_kernels.h", "salec_deck.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "--fmad=false", "-lineinfo",
               "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-warn-spills"]

@@ -91,6 +91,7 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_stream": ([vp, ctypes.POINTER(vp)], c_i),
             "salec_gpu_profile": ([vp, c_i], c_i),
             "salec_gpu_phase_times": ([vp, P_D, ctypes.POINTER(c_ll)], c_i),
+            "salec_cfl_dt_noalloc": ([c_i, c_i, vp, vp, vp, vp, vp, vp, c_d, c_d, vp, vp], c_i),
             "salec_boundary_map": ([c_i, c_i, c_i, c_i, c_i, ctypes.POINTER(c_i), ctypes.POINTER(c_i),
                                     ctypes.POINTER(c_i), ctypes.POINTER(c_i), ctypes.POINTER(ctypes.c_uint)], c_i),
             "salec_gpu_last_error": ([], ctypes.c_char_p),
@@ -143,6 +144,13 @@ def boundary_map(kind: int, pattern: int, nx: int, ny: int, ncomp: int, go: Sequ
                                     src.ctypes.data_as(ip), ops.ctypes.data_as(ctypes.POINTER(ctypes.c_uint))),
            "boundary_map")
     return dst[: n.value], src[: n.value], ops[: n.value]
+
+
+def cfl_dt_noalloc(nx: int, ny: int, vel_r: int, vel_z: int, csd: int, scale_r: int, scale_z: int,
+                   vof_vacuum: int, dt_prev: float, max_dt: float, dt_out: int, stream: int = 0) -> None:
+    """Enqueue the allocation-free CFL reduction; every pointer argument is a device address."""
+    _check(lib().salec_cfl_dt_noalloc(nx, ny, vel_r, vel_z, csd, scale_r, scale_z, vof_vacuum, float(dt_prev),
+                                      float(max_dt), dt_out, stream or None), "salec_cfl_dt_noalloc")
 
 
 def apply_boundary_map(field: np.ndarray, dst, src, ops) -> np.ndarray:
