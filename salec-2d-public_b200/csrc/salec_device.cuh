@@ -338,9 +338,12 @@ __device__ __forceinline__ double ice_melt(double p)
 }
 
 // The registry of src/strength.c:860-875 as one dispatcher. pa = {pressure, damage, plastic
-// strain, strain rate, temperature, ...} (porosity uses its own six arguments).
-static __device__ __noinline__ double strength_fn(int id, const double *pa, const DevMat &s)
+// strain, strain rate, temperature, ...} (porosity uses its own six arguments); passed by value
+// so that no caller keeps an array in local memory.
+static __device__ __noinline__ double strength_fn(int id, double p0, double p1, double p2, double p3, double p4,
+                                                  double p5, const DevMat &s)
 {
+    const double pa[6] = {p0, p1, p2, p3, p4, p5};
     const double BETA = 0.57735026918962576451;   // JohnsonCook factor as in interpolate_fn.h
     switch (id) {
     case 0: { // SimpleRock (never selectable in the reference: str2func rejects index 0)

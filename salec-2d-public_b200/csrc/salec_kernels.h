@@ -57,8 +57,6 @@ __global__ void k_vertex_acceleration(const Ctx c);
 __global__ void k_vertex_displacement(const Ctx c);
 __global__ void k_energy(const Ctx c);
 __global__ void k_tracers(const Ctx c);
-__global__ void k_flux(const Ctx c, int pass);
-__global__ void k_remap_damp_state(const Ctx c, int do_remap, int do_damp, int do_ejecta, int do_state);
 __global__ void k_cycle(const Ctx c);
 __global__ void k_record_reference_state(const Ctx c);
 __global__ void k_init_vertex_velocity(const Ctx c);
@@ -66,6 +64,9 @@ __global__ void k_gather(GatherBatch g, int mode, double *scratch);
 __global__ void k_aos_to_planes(const double *aos, double *base, long long plane, int P, int nx, int ny, int nc);
 __global__ void k_planes_to_aos(const double *base, double *aos, long long plane, int P, int nx, int ny, int nc);
 __global__ void k_count_nonfinite(const double *base, long long n, unsigned long long *out);
+void launch_flux(const Ctx &c, int pass, dim3 g, dim3 b, cudaStream_t s);
+void launch_remap_damp_state(const Ctx &c, int do_remap, int do_damp, int do_ejecta, int do_state, dim3 g, dim3 b,
+                             cudaStream_t s);
 #endif
 
 } // namespace salec

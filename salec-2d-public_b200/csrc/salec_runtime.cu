@@ -267,14 +267,14 @@ int run_phase(salec_gpu *h, int ph)
         if (h->tr.n > 0) k_tracers<<<(h->tr.n + 127) / 128, 128, 0, s>>>(c);
         break;
     case 12:
-        k_flux<<<gc, blk, 0, s>>>(c, 0);
+        launch_flux(c, 0, gc, blk, s);
         rc = run_gather(h, h->g_flux_state);
-        k_flux<<<gc, blk, 0, s>>>(c, 1);
+        launch_flux(c, 1, gc, blk, s);
         break;
     case 13: break;   // strength condition from tracers (lubrication is rejected at create)
     case 14: {
         const int ejecta = (h->rp.flow_resistance > 0. || h->rp.flow_friction > 0.) ? 1 : 0;
-        k_remap_damp_state<<<gc, blk, 0, s>>>(c, 1, 1, ejecta, 1);
+        launch_remap_damp_state(c, 1, 1, ejecta, 1, gc, blk, s);
         break;
     }
     case 15: k_cycle<<<1, 32, 0, s>>>(c); break;
@@ -421,7 +421,7 @@ int salec_internal_finish_init(salec_gpu *h, double damp_time_in, double *damp_t
     const Ctx c = h->ctx();
     const dim3 blk(32, 8);
     const dim3 gc = grid2(h->d.enx, h->d.eny, blk), gv = grid2(h->d.vnx, h->d.vny, blk);
-    k_remap_damp_state<<<gc, blk, 0, h->stream>>>(c, 0, 0, 0, 1);
+    launch_remap_damp_state(c, 0, 0, 0, 1, gc, blk, h->stream);
     int rc = run_gather(h, h->g_init);
     if (rc) return rc;
     CUDA_TRY(cudaMemsetAsync(&h->scal->aux, 0, sizeof(unsigned long long), h->stream));

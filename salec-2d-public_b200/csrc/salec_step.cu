@@ -416,20 +416,18 @@ __global__ void k_stress(const Ctx c)
             const double vm = PLN(c.f.m_vof, m)[p];
             if (vm < SALEC_TOLVOF) continue;
             const DevMat &s = c.mat[m];
-            double pa[6] = {pre, dam, tps, sta2s, tem, 0.};
-            double my = strength_fn(s.yfunc, pa, s);
+            double my = strength_fn(s.yfunc, pre, dam, tps, sta2s, tem, 0., s);
             if (c.rp.acoustic_fluid && pre >= 0.) {
                 const double vibp = dmin(rho * c.f.e_csd[p] * sqrt(c.f.e_vib[p]), pre);
                 const double tm = simon_melt(pre, s);
                 double soft = ohnaka_soft(tem, s, tm);
                 soft = wind(soft, 0.0, 1.0);
                 const double lp = pre - vibp * dam * dam * sqrt(soft);
-                double pb[6] = {lp, dam, tps, sta2s, tem, 0.};
-                const double myv = strength_fn(s.yfunc, pb, s) + rho * s.Acvis * sta2s;
+                const double myv = strength_fn(s.yfunc, lp, dam, tps, sta2s, tem, 0., s) + rho * s.Acvis * sta2s;
                 my = dmin(myv, my);
             }
             shear += vm * dmax(my, 0.0);
-            if (c.rp.tensile_failure) tensile += vm * strength_fn(s.tfunc, pa, s);
+            if (c.rp.tensile_failure) tensile += vm * strength_fn(s.tfunc, pre, dam, tps, sta2s, tem, 0., s);
         }
         if (c.rp.tracer_lubrication >= 1 && c.f.e_cnd[p] >= 1.0) {
             const double lub = dmin(pre * c.rp.tracer_lub_frac + c.rp.tracer_lub_y0, 0.0);
@@ -444,8 +442,7 @@ __global__ void k_stress(const Ctx c)
             double dsd = 0.;
             for (int m = 1; m < nmat; ++m) {
                 const DevMat &s = c.mat[m];
-                double pa[6] = {pre, dam, 0., 0., 0., 0.};
-                dsd += PLN(c.f.m_vof, m)[p] * strength_fn(s.dsdf, pa, s);
+                dsd += PLN(c.f.m_vof, m)[p] * strength_fn(s.dsdf, pre, dam, 0., 0., 0., 0., s);
             }
             dam = wind(dam + sta2s * dsd * dt, 0.0, 1.0);
             tps = dmin(tps + sta2s * dt, 10.);
@@ -632,8 +629,8 @@ __global__ void k_energy(const Ctx c)
                 double *pt = PLN(c.f.m_pty, m) + p;
                 double dpty = 0.;
                 if (c.f.e_sigma[p] + PLN(c.f.e_sigma, 1)[p] <= 0.) {
-                    double pa[6] = {*pt, cvs, pre, dcvs, c.f.e_vel[p], PLN(c.f.e_vel, 1)[p]};
-                    dpty = strength_fn(c.mat[m].porfunc, pa, c.mat[m]);
+                    dpty = strength_fn(c.mat[m].porfunc, *pt, cvs, pre, dcvs, c.f.e_vel[p], PLN(c.f.e_vel, 1)[p],
+                                       c.mat[m]);
                 }
                 *pt += dpty * dt;
                 *pt = wind(*pt, 1.0, c.mat[m].alphamax2);
@@ -806,17 +803,56 @@ __device__ __forceinline__ double algebraic_ratio(double vu, double vd, double v
     return vu + mstacs(nd, gf, cr) * (va - vu);
 }
 
+// Upwind record of one face of cell p (_calculate_flux_set_bphi, src/advect.c:1138-1223): the
+// face is written by the cell it flows out of; a face with zero swept volume gets zero material
+// volumes (see k_flux).
+template <int NM, bool POR, int MM>
+__device__ __forceinline__ void store_face(const Ctx &c, double *f, double vol, const double (&flux)[MM][4], int k,
+                                           long long p, int nmat)
+{
+    if (vol > 0.) return;
+    const long long PL = c.d.PL;
+    if (vol == 0.) {
+#pragma unroll
+        for (int m = 0; m < nmat; ++m) f[m * PL] = 0.0;
+        return;
+    }
+#pragma unroll
+    for (int m = 0; m < nmat; ++m) {
+        f[m * PL] = flux[m][k];
+        f[(m + nmat) * PL] = PLN(c.f.m_den, m)[p];
+        f[(m + 2 * nmat) * PL] = PLN(c.f.m_eng, m)[p];
+    }
+    const int b = 3 * nmat;
+    f[(b + 0) * PL] = c.f.e_vel[p];
+    f[(b + 1) * PL] = PLN(c.f.e_vel, 1)[p];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) f[(b + 2 + q) * PL] = 1.0 * PLN(c.f.e_ste, q)[p];
+    f[(b + 6) * PL] = 1.0 * c.f.e_dam[p];
+    f[(b + 7) * PL] = 1.0 * c.f.e_tps[p];
+    f[(b + 8) * PL] = 1.0 * c.f.e_vib[p];
+    f[(b + 9) * PL] = 1.0 * c.f.e_ejt[p];
+    if (POR) {
+        f[(b + 10) * PL] = 1.0 * c.f.e_cvs[p];
+#pragma unroll
+        for (int m = 0; m < nmat; ++m) f[(b + 11 + m) * PL] = PLN(c.f.m_pty, m)[p];
+    }
+}
+
 // pass 0: interior cells; pass 1: pad cells (after the ghost fills of m_den, m_eng, ...).
-__global__ void k_flux(const Ctx c, int pass)
+template <int NM, bool POR>
+__global__ void __launch_bounds__(256) k_flux(const Ctx c, int pass)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= c.d.enx || j >= c.d.eny) return;
     const bool interior = cell_interior(c, i, j);
     if ((pass == 0) != interior) return;
-    const int nmat = c.d.nmat;
+    constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
+    const int nmat = NM > 0 ? NM : c.d.nmat;
     const long long p = KIDX(i, j);
     const long long vl[4] = {KIDX(i, j), KIDX(i + 1, j), KIDX(i + 1, j + 1), KIDX(i, j + 1)};
     double px[4], py[4], dx[4], dy[4];
+    #pragma unroll
     for (int k = 0; k < 4; ++k) {
         px[k] = c.f.v_pos[vl[k]]; py[k] = PLN(c.f.v_pos, 1)[vl[k]];
         dx[k] = c.f.v_dis[vl[k]]; dy[k] = PLN(c.f.v_dis, 1)[vl[k]];
@@ -827,44 +863,61 @@ __global__ void k_flux(const Ctx c, int pass)
     const double uv = swept_volume(px[3], py[3], px[2], py[2], dx[3], dy[3], dx[2], dy[2]);
     const double lbru[4] = {lv, bv, rv, uv};
 
-    double vof[SALEC_MAXMAT];
+    double vof[MM];
+    #pragma unroll
     for (int m = 0; m < nmat; ++m) vof[m] = PLN(c.f.m_vof, m)[p];
     const double evol = c.f.e_vol[p];
-    double flux[SALEC_MAXMAT][4];
+    double flux[MM][4];
+    #pragma unroll
     for (int m = 0; m < nmat; ++m) flux[m][0] = flux[m][1] = flux[m][2] = flux[m][3] = 0.;
 
+    // primary material: vacuum, or the largest fraction when the cell holds no vacuum; selected
+    // with compare loops so that the per-material arrays stay in registers
     int prim = 0;
-    if (vof[0] < SALEC_TOLVOF)
+    double vprim = vof[0];
+    if (vof[0] < SALEC_TOLVOF) {
+#pragma unroll
         for (int m = 1; m < nmat; ++m)
-            if (vof[m] > vof[prim]) prim = m;
+            if (vof[m] > vprim) { prim = m; vprim = vof[m]; }
+    }
 
     double wpt[4];
-    if (vof[prim] > 1.0 - SALEC_TOLVOF) {
-        flux[prim][0] = dmin(lv, 0);
-        flux[prim][2] = -1.0 * dmin(rv, 0);
-        flux[prim][1] = dmin(bv, 0);
-        flux[prim][3] = -1.0 * dmin(uv, 0);
+    if (vprim > 1.0 - SALEC_TOLVOF) {
+#pragma unroll
+        for (int m = 0; m < nmat; ++m)
+            if (m == prim) {
+                flux[m][0] = dmin(lv, 0);
+                flux[m][2] = -1.0 * dmin(rv, 0);
+                flux[m][1] = dmin(bv, 0);
+                flux[m][3] = -1.0 * dmin(uv, 0);
+            }
         const double w = prim == 0 ? 1.0 : -0.25;
         wpt[0] = wpt[1] = wpt[2] = wpt[3] = w;
     } else {
         double grd[12];
+        #pragma unroll
         for (int k = 0; k < 8; ++k) grd[k] = PLN(c.f.e_grad, k)[p];
         double gx = 0., gy = 0.;
         {
             const double *vv = PLN(c.f.v_vof, prim);
             double vq[4];
+            #pragma unroll
             for (int k = 0; k < 4; ++k) vq[k] = vv[vl[k]];
+            #pragma unroll
             for (int k = 0; k < 4; ++k) gx += vq[k] * grd[k];
+            #pragma unroll
             for (int k = 0; k < 4; ++k) gy += vq[k] * grd[4 + k];
         }
         normalise2(gx, gy);
         double ca = PLN(c.f.e_pos, 2)[p] * fabs(gx);
         double cb = PLN(c.f.e_pos, 3)[p] * fabs(gy);
         if (ca < cb) { double t = ca; ca = cb; cb = t; }
-        const double dstar = cut_length(vof[prim], ca, cb);
+        const double dstar = cut_length(vprim, ca, cb);
         double lw[4];
+        #pragma unroll
         for (int k = 0; k < 4; ++k) { double s = 0.; s += gx * px[k]; s += gy * py[k]; lw[k] = s; }
         const double mw = dmax(dmax(lw[0], lw[1]), dmax(lw[2], lw[3]));
+        #pragma unroll
         for (int k = 0; k < 4; ++k) lw[k] = lw[k] - mw + dstar;
         if (prim == 0) { for (int k = 0; k < 4; ++k) wpt[k] = lw[k]; }
         else wpt[0] = wpt[1] = wpt[2] = wpt[3] = -0.25;
@@ -888,33 +941,43 @@ __global__ void k_flux(const Ctx c, int pass)
         fnx[2] = c.f.bx_normal[fb[2]]; fny[2] = PLN(c.f.bx_normal, 1)[fb[2]];
         fnx[1] = c.f.by_normal[fb[1]]; fny[1] = PLN(c.f.by_normal, 1)[fb[1]];
         fnx[3] = c.f.by_normal[fb[3]]; fny[3] = PLN(c.f.by_normal, 1)[fb[3]];
-        double fnp[SALEC_MAXMAT][4];
+        double fnp[MM][4];
         double snp[4] = {0., 0., 0., 0.};
+        #pragma unroll
         for (int m = 0; m < nmat; ++m) fnp[m][0] = fnp[m][1] = fnp[m][2] = fnp[m][3] = 0.;
+        #pragma unroll
         for (int m = 1; m < nmat; ++m) {
             if (m == prim) continue;
             const double *vv = PLN(c.f.v_vof, m);
             double vq[4];
+            #pragma unroll
             for (int k = 0; k < 4; ++k) vq[k] = vv[vl[k]];
             double ngx = 0., ngy = 0.;
+            #pragma unroll
             for (int k = 0; k < 4; ++k) ngx += vq[k] * grd[k];
+            #pragma unroll
             for (int k = 0; k < 4; ++k) ngy += vq[k] * grd[4 + k];
             normalise2(ngx, ngy);
             const double *ev = PLN(c.f.m_vof, m);
             const double up[4] = {ev[nb[0]], ev[nb[1]], ev[nb[2]], ev[nb[3]]};
             const double ac[4] = {up[2], up[3], up[0], up[1]};
+            #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 fnp[m][k] = algebraic_ratio(up[k], vof[m], ac[k], cr, fnx[k], fny[k], ngx, ngy);
                 snp[k] += fnp[m][k];
             }
         }
+        #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (snp[k] > SALEC_TOLVOF) {
+                #pragma unroll
                 for (int m = 1; m < nmat; ++m) fnp[m][k] = fnp[m][k] / snp[k];
             } else {
-                for (int m = 1; m < nmat; ++m) fnp[m][k] = vof[m] / (1.0 - vof[prim]);
+                #pragma unroll
+                for (int m = 1; m < nmat; ++m) fnp[m][k] = vof[m] / (1.0 - vprim);
             }
         }
+        #pragma unroll
         for (int m = 0; m < nmat; ++m) {
             if (m == prim) {
                 flux[m][0] = dmin(lv, 0.0) * fp[0];
@@ -929,70 +992,51 @@ __global__ void k_flux(const Ctx c, int pass)
             }
         }
     }
+    #pragma unroll
     for (int k = 0; k < 4; ++k) PLN(c.f.e_wpt, k)[p] = wpt[k];
 
     // cap the out-flux of each material by its content
+    #pragma unroll
     for (int m = 1; m < nmat; ++m) {
         double d = 0.;
         d += flux[m][0] * 1.0; d += flux[m][1] * 1.0; d += flux[m][2] * -1.0; d += flux[m][3] * -1.0;
         const double out = -1.0 * d;
         if (out > vof[m] * evol) {
             const double s = vof[m] * evol / out;
+            #pragma unroll
             for (int k = 0; k < 4; ++k) flux[m][k] *= s;
         }
     }
 
     // faces l, b, r, u
-    const long long PL = c.d.PL;
-    double *face[4] = {c.f.bx_phi + KIDX(i, j), c.f.by_phi + KIDX(i, j), c.f.bx_phi + KIDX(i + 1, j),
-                       c.f.by_phi + KIDX(i, j + 1)};
-    const int phi = c.d.phi;
-    for (int k = 0; k < 4; ++k) {
-        if (lbru[k] > 0.) continue;
-        double *f = face[k];
-        if (lbru[k] == 0.) {
-            for (int m = 0; m < nmat; ++m) f[m * PL] = 0.0;
-            continue;
-        }
-        for (int m = 0; m < nmat; ++m) {
-            f[m * PL] = flux[m][k];
-            f[(m + nmat) * PL] = PLN(c.f.m_den, m)[p];
-            f[(m + 2 * nmat) * PL] = PLN(c.f.m_eng, m)[p];
-        }
-        const int b = 3 * nmat;
-        f[(b + 0) * PL] = c.f.e_vel[p];
-        f[(b + 1) * PL] = PLN(c.f.e_vel, 1)[p];
-        for (int q = 0; q < 4; ++q) f[(b + 2 + q) * PL] = 1.0 * PLN(c.f.e_ste, q)[p];
-        f[(b + 6) * PL] = 1.0 * c.f.e_dam[p];
-        f[(b + 7) * PL] = 1.0 * c.f.e_tps[p];
-        f[(b + 8) * PL] = 1.0 * c.f.e_vib[p];
-        f[(b + 9) * PL] = 1.0 * c.f.e_ejt[p];
-        if (c.rp.porosity_model) {
-            f[(b + 10) * PL] = 1.0 * c.f.e_cvs[p];
-            for (int m = 0; m < nmat; ++m) f[(b + 11 + m) * PL] = PLN(c.f.m_pty, m)[p];
-        }
-        (void)phi;
-    }
+    store_face<NM, POR>(c, c.f.bx_phi + KIDX(i, j), lv, flux, 0, p, nmat);
+    store_face<NM, POR>(c, c.f.by_phi + KIDX(i, j), bv, flux, 1, p, nmat);
+    store_face<NM, POR>(c, c.f.bx_phi + KIDX(i + 1, j), rv, flux, 2, p, nmat);
+    store_face<NM, POR>(c, c.f.by_phi + KIDX(i, j + 1), uv, flux, 3, p, nmat);
 }
 
 // ============================================================ phase 14: remap + damping + EOS
 // advect_flux_default (src/advect.c:26-302), damp_on_cell (src/velocity.c:356-767),
 // ejecta_flow (src/ejecta.c:65-133) and update_state (src/sale2d.c:1635-1742), fused per cell:
 // the damping reads only its own cell, and the EOS reads the damped material state.
-__device__ void remap_cell(const Ctx &c, int i, int j, long long p)
+template <int NM, bool POR>
+__device__ __forceinline__ void remap_cell(const Ctx &c, int i, int j, long long p)
 {
-    const int nmat = c.d.nmat;
-    const int phi = c.d.phi;
+    constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
+    const int nmat = NM > 0 ? NM : c.d.nmat;
+    const int phi = 3 * nmat + 10 + (POR ? nmat + 1 : 0);
     const long long PL = c.d.PL;
-    const bool por = c.rp.porosity_model != 0;
+    constexpr bool por = POR;
     const double *face[4] = {c.f.bx_phi + KIDX(i, j), c.f.by_phi + KIDX(i, j), c.f.bx_phi + KIDX(i + 1, j),
                              c.f.by_phi + KIDX(i, j + 1)};
     const double dir[4] = {1.0, 1.0, -1.0, -1.0};
-    double dphi[4 * SALEC_MAXMAT + 11];
+    double dphi[4 * MM + 11];
+    #pragma unroll
     for (int q = 0; q < phi; ++q) dphi[q] = 0.;
     const int b = 3 * nmat;
     for (int k = 0; k < 4; ++k) {
         const double *f = face[k];
+        #pragma unroll
         for (int m = 0; m < nmat; ++m) {
             const double mv = dir[k] * f[m * PL];
             if (mv == 0.0) continue;   // adds only signed zeros to dphi (see k_flux)
@@ -1001,6 +1045,7 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
             dphi[m + nmat] += mv * rho_f;
             dphi[m + 2 * nmat] += mv * f[(m + 2 * nmat) * PL];
             const double fm = mv * rho_f;
+            #pragma unroll
             for (int q = 0; q < 10; ++q) dphi[b + q] += fm * f[(b + q) * PL];
             if (por) {
                 dphi[b + 10] += (f[(b + 10) * PL]) * (mv * rho_f);
@@ -1008,7 +1053,8 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
             }
         }
     }
-    double vof[SALEC_MAXMAT], rho[SALEC_MAXMAT], eng[SALEC_MAXMAT], pty[SALEC_MAXMAT];
+    double vof[MM], rho[MM], eng[MM], pty[MM];
+    #pragma unroll
     for (int m = 0; m < nmat; ++m) {
         vof[m] = PLN(c.f.m_vof, m)[p];
         rho[m] = PLN(c.f.m_den, m)[p];
@@ -1017,13 +1063,16 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
     }
     const double evol = c.f.e_vol[p];
     double emass = evol * c.f.e_den[p];
-    double sphi[4 * SALEC_MAXMAT + 11];
+    double sphi[4 * MM + 11];
+    #pragma unroll
     for (int q = 0; q < phi; ++q) sphi[q] = 0.;
+    #pragma unroll
     for (int m = 0; m < nmat; ++m) {
         sphi[m] += vof[m] * evol;
         sphi[m + nmat] += vof[m] * evol * rho[m];
         sphi[m + 2 * nmat] += vof[m] * evol * eng[m];
     }
+    #pragma unroll
     for (int q = 0; q < 4; ++q) sphi[b + 2 + q] += emass * PLN(c.f.e_ste, q)[p];
     sphi[b + 6] = emass * c.f.e_dam[p];
     sphi[b + 7] = emass * c.f.e_tps[p];
@@ -1031,11 +1080,14 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
     sphi[b + 9] = emass * c.f.e_ejt[p];
     if (por) {
         sphi[b + 10] = emass * c.f.e_cvs[p];
+        #pragma unroll
         for (int m = 0; m < nmat; ++m) sphi[b + 11 + m] = vof[m] * evol * rho[m] * pty[m];
     }
+    #pragma unroll
     for (int q = 0; q < phi; ++q) sphi[q] += 1.0 * dphi[q];
     double zeta = 0.0;
     emass = 0.;
+    #pragma unroll
     for (int m = 0; m < nmat; ++m) {
         if (sphi[m] < 0.) { sphi[m] = 0.; sphi[m + nmat] = 0.; }
         if (m == 0) continue;
@@ -1044,19 +1096,24 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
     }
     if (zeta > evol * (1.0 - SALEC_TOLVOF) || (zeta > 0. && sphi[0] < evol * SALEC_TOLVOF)) {
         const double s = 1.0 / zeta;
+        #pragma unroll
         for (int m = 0; m < nmat; ++m) vof[m] = s * sphi[m];
         vof[0] = 0.0;
     } else if (zeta < evol * SALEC_TOLVOF) {
+        #pragma unroll
         for (int m = 0; m < nmat; ++m) vof[m] = 0.;
         vof[0] = 1.0;
     } else if (c.rp.partpres) {
         const double s = 1.0 / (zeta + sphi[0]);
+        #pragma unroll
         for (int m = 0; m < nmat; ++m) vof[m] = s * sphi[m];
     } else {
         sphi[0] = evol - zeta;
         const double s = 1.0 / evol;
+        #pragma unroll
         for (int m = 0; m < nmat; ++m) vof[m] = s * sphi[m];
     }
+    #pragma unroll
     for (int m = 1; m < nmat; ++m) {
         if (vof[m] < SALEC_TOLVOF || sphi[m + nmat] < SALEC_TOLRHO * SALEC_TOLVOF * evol) {
             eng[m] = 0.0; rho[m] = 0.0; vof[m] = 0.0;
@@ -1071,6 +1128,7 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
     if (emass > SALEC_TOLRHO * evol) {
         const double s = 1.0 / emass;
         dvx = s * sphi[b]; dvy = s * sphi[b + 1];
+        #pragma unroll
         for (int q = 0; q < 4; ++q) st[q] = s * sphi[b + 2 + q];
         dam = sphi[b + 6] / emass;
         tps = sphi[b + 7] / emass;
@@ -1088,8 +1146,10 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
     dam = wind(dam, 0.0, 1.0);
     ejt = wind(ejt, 0.0, 1.0);
     if (por)
+        #pragma unroll
         for (int m = 1; m < nmat; ++m) pty[m] = wind(pty[m], 1.0, c.mat[m].alphamax2);
     if (eden < c.rp.density_cutoff || eden < 10.0 * c.rp.density_cutoff * (1.0 - vof[0])) {
+        #pragma unroll
         for (int m = 0; m < nmat; ++m) { vof[m] = 0.; rho[m] = 0.; eng[m] = 0.; }
         vof[0] = 1.0;
         dvx = dvy = 0.;
@@ -1097,9 +1157,11 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
         dam = tps = vib = ejt = 0.;
         if (por) {
             cvs = 0.;
+            #pragma unroll
             for (int m = 1; m < nmat; ++m) pty[m] = 1.0;
         }
     }
+    #pragma unroll
     for (int m = 0; m < nmat; ++m) {
         PLN(c.f.m_vof, m)[p] = vof[m];
         PLN(c.f.m_den, m)[p] = rho[m];
@@ -1108,6 +1170,7 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
     }
     c.f.e_dvel[p] = dvx;
     PLN(c.f.e_dvel, 1)[p] = dvy;
+    #pragma unroll
     for (int q = 0; q < 4; ++q) PLN(c.f.e_ste, q)[p] = st[q];
     c.f.e_dam[p] = dam;
     c.f.e_tps[p] = tps;
@@ -1117,15 +1180,16 @@ __device__ void remap_cell(const Ctx &c, int i, int j, long long p)
     c.f.e_den[p] = eden;
 }
 
-__device__ void damp_cell(const Ctx &c, long long p, double dt)
+template <int NM, bool POR>
+__device__ __forceinline__ void damp_cell(const Ctx &c, long long p, double dt)
 {
-    const int nmat = c.d.nmat;
+    const int nmat = NM > 0 ? NM : c.d.nmat;
     const int ty = c.rp.damp_type;
     if (ty == 4 || ty == 5) return;
     if (c.f.m_vof[p] > SALEC_TOLVOF) return;
     const double sx = c.f.e_sigma[p], sy = PLN(c.f.e_sigma, 1)[p];
     const double d0 = c.f.e_dampref[p], d1 = PLN(c.f.e_dampref, 1)[p];
-    const bool por = c.rp.porosity_model != 0;
+    constexpr bool por = POR;
     if (ty == 0) {
         // damp_on_cell_pml (src/velocity.c:378-467)
         double ax = c.f.e_alpha[p], ay = PLN(c.f.e_alpha, 1)[p];
@@ -1133,6 +1197,7 @@ __device__ void damp_cell(const Ctx &c, long long p, double dt)
         if (sy > 0.0) {
             ay += (sy * PLN(c.f.e_grad_vel, 0)[p] + sy * PLN(c.f.e_grad_vel, 4)[p] - c.rp.alpha_damp_y * ay) * dt;
             PLN(c.f.e_dvel, 1)[p] += -1.0 * sy * PLN(c.f.e_vel, 1)[p] * dt;
+            #pragma unroll
             for (int m = 1; m < nmat; ++m) {
                 if (PLN(c.f.m_vof, m)[p] < 1.0 - SALEC_TOLVOF) continue;
                 double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
@@ -1147,6 +1212,7 @@ __device__ void damp_cell(const Ctx &c, long long p, double dt)
         if (sx > 0.0) {
             ax += (sx * PLN(c.f.e_grad_vel, 3)[p] + sx * PLN(c.f.e_grad_vel, 4)[p] - c.rp.alpha_damp_x * ax) * dt;
             c.f.e_dvel[p] += -1.0 * sx * c.f.e_vel[p] * dt;
+            #pragma unroll
             for (int m = 1; m < nmat; ++m) {
                 if (PLN(c.f.m_vof, m)[p] > 1.0 - SALEC_TOLVOF) {
                     double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
@@ -1178,6 +1244,7 @@ __device__ void damp_cell(const Ctx &c, long long p, double dt)
         ay += -1.0 * sd * dt - 1.0 * (adx + ady) * ay * dt;
         c.f.e_alpha[p] = ax;
         PLN(c.f.e_alpha, 1)[p] = ay;
+        #pragma unroll
         for (int m = 1; m < nmat; ++m) {
             if (PLN(c.f.m_vof, m)[p] < 1.0 - SALEC_TOLVOF) continue;
             double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
@@ -1198,6 +1265,7 @@ __device__ void damp_cell(const Ctx &c, long long p, double dt)
     } else if (ty == 3) {
         // damp_on_cell_sbc (src/velocity.c:658-767); "+=" in y and "=" in x as in the reference
         if (sy < 1.0) {
+            #pragma unroll
             for (int m = 1; m < nmat; ++m) {
                 if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
                 double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
@@ -1207,6 +1275,7 @@ __device__ void damp_cell(const Ctx &c, long long p, double dt)
             }
         }
         if (sx < 1.0) {
+            #pragma unroll
             for (int m = 1; m < nmat; ++m) {
                 if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
                 double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
@@ -1231,6 +1300,7 @@ __device__ void ejecta_drag_cell(const Ctx &c, int i, int j, long long p, double
             PLN(c.f.e_dvel, 1)[p] += -c.rp.flow_resistance * dt * PLN(c.f.e_vel, 1)[p];
         }
         if (c.rp.flow_friction > 0.) {
+            #pragma unroll
             for (int q = 0; q < 4; ++q) PLN(c.f.e_ste, q)[p] = 0.;
             if (c.f.e_vel[p] >= 0.) c.f.e_dvel[p] += -1.0 * c.rp.flow_friction * fabs(gyy) * dt;
             else c.f.e_dvel[p] += 1.0 * c.rp.flow_friction * fabs(gyy) * dt;
@@ -1238,13 +1308,16 @@ __device__ void ejecta_drag_cell(const Ctx &c, int i, int j, long long p, double
     }
 }
 
-__device__ void state_cell(const Ctx &c, long long p)
+template <int NM, bool POR>
+__device__ __forceinline__ void state_cell(const Ctx &c, long long p)
 {
-    const int nmat = c.d.nmat;
-    const bool por = c.rp.porosity_model != 0;
+    constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
+    const int nmat = NM > 0 ? NM : c.d.nmat;
+    constexpr bool por = POR;
     const double dam = c.f.e_dam[p];
-    double mpre[SALEC_MAXMAT], mcsd[SALEC_MAXMAT], mtem[SALEC_MAXMAT];
+    double mpre[MM], mcsd[MM], mtem[MM];
     double epre = 0.0, ecsd = 0.0, etem = 0.0, eden = 0.0, emu = 0.0;
+    #pragma unroll
     for (int m = 1; m < nmat; ++m) {
         const double vm = PLN(c.f.m_vof, m)[p];
         if (vm < SALEC_TOLVOF) {
@@ -1256,6 +1329,7 @@ __device__ void state_cell(const Ctx &c, long long p)
             material_state(s, PLN(c.f.m_den, m)[p], PLN(c.f.m_eng, m)[p], plim, pt, mtem[m], mpre[m], mcsd[m]);
         }
     }
+    #pragma unroll
     for (int m = 1; m < nmat; ++m) {
         const double vm = PLN(c.f.m_vof, m)[p];
         const double rm = PLN(c.f.m_den, m)[p];
@@ -1284,17 +1358,44 @@ __device__ void state_cell(const Ctx &c, long long p)
     c.f.e_mu[p] = emu;
 }
 
-__global__ void k_remap_damp_state(const Ctx c, int do_remap, int do_damp, int do_ejecta, int do_state)
+template <int NM, bool POR>
+__global__ void __launch_bounds__(256) k_remap_damp_state(const Ctx c, int do_remap, int do_damp, int do_ejecta, int do_state)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= c.d.enx || j >= c.d.eny) return;
     const long long p = KIDX(i, j);
     const bool interior = cell_interior(c, i, j);
     const double dt = c.scal->dt;
-    if (do_remap && interior) remap_cell(c, i, j, p);
-    if (do_damp && c.rp.damp_time > c.scal->time) damp_cell(c, p, dt);
+    if (do_remap && interior) remap_cell<NM, POR>(c, i, j, p);
+    if (do_damp && c.rp.damp_time > c.scal->time) damp_cell<NM, POR>(c, p, dt);
     if (do_ejecta && interior) ejecta_drag_cell(c, i, j, p, dt);
-    if (do_state && interior) state_cell(c, p);
+    if (do_state && interior) state_cell<NM, POR>(c, p);
+}
+
+// Launchers: the material count and the porosity switch are template parameters, so that the
+// per-material and per-record arrays of the flux and remap kernels are fully unrolled into
+// registers for the common material counts; other counts use the generic instance.
+#define SALEC_NM_DISPATCH(KERNEL, ...)                                                             \
+    do {                                                                                           \
+        const bool por_ = c.rp.porosity_model != 0;                                                \
+        switch (c.d.nmat) {                                                                        \
+        case 2: if (por_) KERNEL<2, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<2, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        case 3: if (por_) KERNEL<3, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<3, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        case 4: if (por_) KERNEL<4, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<4, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        case 5: if (por_) KERNEL<5, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<5, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        default: if (por_) KERNEL<0, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<0, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        }                                                                                          \
+    } while (0)
+
+void launch_flux(const Ctx &c, int pass, dim3 g, dim3 b, cudaStream_t s)
+{
+    SALEC_NM_DISPATCH(k_flux, c, pass);
+}
+
+void launch_remap_damp_state(const Ctx &c, int do_remap, int do_damp, int do_ejecta, int do_state, dim3 g, dim3 b,
+                             cudaStream_t s)
+{
+    SALEC_NM_DISPATCH(k_remap_damp_state, c, do_remap, do_damp, do_ejecta, do_state);
 }
 
 // ============================================================ phase 15: cycle control

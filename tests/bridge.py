@@ -125,6 +125,8 @@ def small_deck(kind: str = "base") -> decks.Deck:
     """Small decks covering the reference's branches (CPU oracle init in ~20 s each)."""
     if kind == "base":
         return decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damp_x=4, damp_y=4)
+    if kind == "tiny":
+        return decks.Deck(npx=12, npy=16, radius_cells=3, maxstep=40, damp_x=3, damp_y=3)
     if kind == "pml2_acfl":
         d = decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damping="pml2", damp_x=4, damp_y=4)
         d.materials = [decks.Material("basalt_", toff=16.0, block_size=200.0)]
