@@ -38,36 +38,74 @@ METRIC = "cell-updates/s"
 WORKLOAD = "impact 2048x2048 cells, SieDen granite + Tillotson ice, CPPR 40, 15 km/s, PML 30, FP64"
 
 # ---------------------------------------------------------------- algorithmic bytes model
-# Doubles that each step kernel must read and write once per point of its domain (fields
-# touched x components, read and write counted separately). "c" = interior cells, "C" = all
-# cells, "v" = active vertices; m = materials (with vacuum), phi = face record length.
-def phase_doubles(m: int, phi: int, pml2: bool):
-    return {
-        0: [("C", 1 + 1 + 2)],                                   # vof0, y, e_ejt rw
-        1: [("C", m), ("v", m)],                                 # m_vof -> v_vof
-        2: [("C", 4 + 1 + 2), ("v", 4 + 2 * 2 + 2 * 2)],         # wpt, den, dvel | v_vol, v_vel rw, v_mass rw
-        3: [("c", 1 + 4 + 2), ("v", 2 + 2)],                     # den, wpt, e_vel w | v_mass, v_vel
-        4: [("C", 1 + 4), ("v", 2 * 2)],                         # den, wpt | v_vel rw
-        5: [("c", 12 + 1 + 1 + 1 + 1 + 3 + 1 + 2 + 5 + 1 + 1), ("v", 2)],
-        6: [],
-        7: [("c", m + 1 + 2 * 4 + 2 * 3 + 1 + 1 + 5 + 1 + 1 + 1 + 1)],
-        8: [("v", 4 + 8 + 4 + 9 + 2 + 2 + 1 + 2 + (4 if pml2 else 0)), ("C", 7 + (3 if pml2 else 0))],
-        9: [("v", 2 * 2 + 2 + 2)],
-        10: [("c", m + 1 + 1 + 1 + 1 + 5 + 4 + m + 2 * m + 2)],
-        11: [],
-        12: [("v", 2 + 2 + m), ("C", 8 + m + 1 + 2 + 2 * m + 2 + 4 + 4 + 4), ("f", phi)],
-        13: [],
-        14: [("f", 2 * phi), ("C", 2 * (3 * m) + 1 + 2 * 1 + 2 * 4 + 2 * 4 + 2 + 2 + 3 + 2 * 2 + 3 + 2 + 1 + 4)],
-        15: [],
-    }
+# Bytes that each step kernel must move: every field its sweep reads, once, and every field
+# it writes, once, at each point where the reference's algorithm touches that field (FP64,
+# 8 bytes a value). Point classes, counted on the device state of the timed window:
+#   C  interior cells                 V  active vertices (update + internal sections)
+#   Cf cells holding no vacuum (vof0 <= 1e-6): the only cells whose stress and energy change
+#   Cn cells that are not pure vacuum (vof0 < 1 - 1e-6)
+#   L  damping-layer cells (sigma_x or sigma_y > 0) while t < damp_time
+#   Cp all cells including the two-cell pad (surface profile sweep)
+# Data-dependent extras are NOT counted, so the figures are lower bounds of what a launch
+# needs: the upwind state members of a face record (read and written only on faces that
+# carry flow), the cut-line reconstruction inputs of mixed cells, the void-vertex fills and
+# the boundary gathers. Geometry that the reference stores per point (e_grad, v_vol, v_suf,
+# v_subvol, v_laplace, e_pos, e_vol) is counted, since it is read from HBM, not recomputed.
+def kernel_doubles(ph: int, k: dict, m: int, pml2: bool, damping: bool, porous: bool, acoustic: bool,
+                   ntracers: int) -> float:
+    C, V, Cf, Cn, L, Cp = k["C"], k["V"], k["Cf"], k["Cn"], k["L"], k["Cp"]
+    if ph == 0:    # trace_profile: vof0, centre y
+        return 2 * Cp
+    if ph == 1:    # update_v_vof: m_vof (m) -> v_vof (m), and in the same sweep update_v_vel_inc:
+        return m * C + m * V + 7 * C + 11 * V   # e_wpt 4, e_den, e_dvel 2 | v_vol 4, v_vel rw, v_mass r1 w2
+    if ph == 3:    # update_e_vel: e_den, e_wpt 4, e_vel w2 | v_mass 2, v_vel 2
+        return 7 * C + 4 * V
+    if ph == 4:    # check_v_vel: e_den, e_wpt 4 (fills of void vertices are data-dependent)
+        return 5 * C
+    if ph == 5:    # gradvel + q + CFL: e_grad 12, e_pos 3, e_vol, vof0, csd, pre, den, e_vel 2 | v_vel 2;
+        return 29 * C + 2 * V    # writes e_grad_vel 5, e_div_vel, e_q
+    if ph == 7:    # stress: vof0, dam everywhere; vacuum cells write 7 zeros; full cells read ste 4, ste2s,
+        d = 2 * C + 7 * (C - Cf) + (8 + m + 9 + 9) * Cf   # sta2s, tps, strength, m-1 vof, den, grad_vel 5,
+        #                                                   mu, pre, tem, csd and write 9
+        return d + (4 * Cf if acoustic else 0)
+    if ph == 8:    # acceleration: v_subvol 4, v_suf 8, v_vol 4, v_laplace 9, v_vel 2, v_mass, v_bf 2,
+        return 32 * V + 7 * C + ((4 * V + 3 * C) if pml2 else 0)   # v_acc w2 | e_pre, e_q, e_ste 4, e_den
+    if ph == 9:    # v_dis: v_vel rw, v_acc | v_dis w
+        return 8 * V
+    if ph == 10:   # energy: vof0, den everywhere; full cells pre, q, div, grad_vel 5, ste 4, vof/den (m-1),
+        d = 2 * C + (14 + 4 * (m - 1)) * Cf    # m_eng rw (m-1), e_cvs rw
+        return d + ((2 * (m - 1) + 5) * Cf if porous else 0)
+    if ph == 11:   # tracers: 12 members rw + 4 vertex displacements (2 each)
+        return 32 * ntracers
+    if ph == 12:   # flux: v_pos 2, v_dis 2 | m_vof m, e_vol; writes e_wpt 4 and m face volumes on 2 faces
+        return (3 * m + 5) * C + 4 * V
+    if ph == 14:   # remap: 2m face volumes, state 3m+9 in, 3m+11 out; EOS writes pre, csd, tem, mu;
+        d = (8 * m + 24) * C   # damping reads sigma 2, dampref 2 on non-vacuum cells, 14 more in the layers
+        if porous:
+            d += 3 * (m + 1) * C
+        if damping:
+            d += 4 * Cn + (14 if pml2 else 10) * L
+        return d
+    return 0.0
 
 
-def phase_bytes(ph: int, nx: int, ny: int, m: int, phi: int, pml2: bool) -> float:
-    npts = {"c": nx * ny, "C": (nx + 4) * (ny + 4), "v": (nx + 3) * (ny + 3), "f": (nx + 4) * (ny + 4)}
-    return 8.0 * sum(npts[d] * k for d, k in phase_doubles(m, phi, pml2)[ph])
+def manifest_doubles(m: int, damp_type: int, porous: bool) -> float:
+    """Whole-step lower bound per cell-update: every persistent field read once and written once
+    (1 write for e_strength), read-only fields once, transient inter-phase arrays and separable
+    geometry excluded. Cell rw: m_vof, m_den, m_eng (3m), e_ste 4, e_dvel 2, 12 scalars, e_wpt 4,
+    e_vel 2, e_alpha 2 (pml, pml2, pml3); vertex rw: v_vel, v_acc, v_dis, v_mass (8), v_alpha 2
+    (pml2, pml3); read-only: e_sigma 2, e_dampref 3, m_pty m, v_bf 2."""
+    e_alpha = 2 if damp_type in (0, 1, 2) else 0
+    v_alpha = 2 if damp_type in (1, 2) else 0
+    rw = 3 * m + 4 + 2 + 12 + 4 + 2 + e_alpha + 8 + v_alpha
+    ro = 2 + 3 + m + 2
+    d = 2 * rw + 1 + ro
+    if porous:
+        d += 2 * (m - 1) + 2
+    return d
 
 
-PHASE_KERNELS = {0: "k_trace_profile", 1: "k_vertex_vof", 2: "k_vertex_momentum", 3: "k_cell_velocity",
+PHASE_KERNELS = {0: "k_trace_profile", 1: "k_vertex_vof_momentum", 2: "-", 3: "k_cell_velocity",
                  4: "k_void_vertices", 5: "k_gradient_viscosity_cfl", 6: "k_finalize_dt", 7: "k_stress",
                  8: "k_vertex_acceleration", 9: "k_vertex_displacement", 10: "k_energy", 11: "k_tracers",
                  12: "k_flux", 13: "-", 14: "k_remap_damp_state", 15: "k_cycle"}
@@ -83,15 +121,18 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(kernel: str):
-    """DRAM bytes per launch of a kernel from the committed ncu summary, if present."""
+def profile_traffic(kernel: str, cells: int):
+    """DRAM bytes (read + write) of one launch of a kernel on the full workload, scaled from the
+    committed ncu capture (profiles/ncu_summary.json: bytes per interior cell of the captured
+    case, whose traffic grows in proportion to the cells), or None without a capture."""
     p = os.path.join(ROOT, "profiles", "ncu_summary.json")
     if not os.path.exists(p):
         return None
     try:
         with open(p) as f:
             d = json.load(f)
-        return d.get("dram_bytes_per_launch_full_workload", {}).get(kernel)
+        per_cell = d["dram_bytes_per_cell"].get(kernel)
+        return None if per_cell is None else per_cell * cells
     except Exception:
         return None
 
@@ -113,7 +154,7 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -247,36 +288,61 @@ def run_gpu_arm(args):
     sim.sync()
     stream = torch.cuda.ExternalStream(sim.stream())
     sampler = ClockSampler(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    # timed region: K steps, nothing else on the stream (no per-phase events)
     barrier()
     torch.cuda.synchronize()
     sampler.start()
-    sim.profile(True)
     launches0 = sim.scalar("launches")
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     sim.step(args.steps)
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
-    phase_ms, phase_cnt = sim.phase_times()
     launches = int(sim.scalar("launches") - launches0)
-    sim.profile(False)
     clocks = sampler.stop()
     torch.cuda.synchronize()
     barrier()
     ms_max = all_max(ms)
     value = world * cells * args.steps / (ms_max / 1000.0)
 
+    # per-kernel times: a separate profiled pass (CUDA events around every phase on the
+    # library's stream), right after the timed region
+    prof_steps = min(args.steps, 50)
+    sim.profile(True)
+    sim.step(prof_steps)
+    sim.sync()
+    phase_ms, phase_cnt = sim.phase_times()
+    sim.profile(False)
+
+    # point classes of this state, for the algorithmic bytes of each kernel
+    vof0 = sim.get_field("m_vof")[..., 0][2:-2, 2:-2]
+    sig = sim.get_field("e_sigma")[2:-2, 2:-2]
+    damping = run.damp_type != 5 and run.damp_time > sim.scalar("time")
+    counts = {"C": cells, "V": (n + 3) * (n + 3), "Cp": (n + 4) * (n + 4),
+              "Cf": int(np.count_nonzero(vof0 <= 1e-6)), "Cn": int(np.count_nonzero(vof0 < 1.0 - 1e-6)),
+              "L": int(np.count_nonzero(((sig[..., 0] > 0) | (sig[..., 1] > 0)) & (vof0 < 1.0 - 1e-6)))}
+    ntr = len(sim.get_tracers())
+    kd = {p: kernel_doubles(p, counts, nmat, pml2, damping, bool(run.porosity_model), bool(run.acoustic_fluid),
+                            ntr) for p in range(16)}
+
     # dominant kernel and its roofline
     hbm, peak_kind = load_peaks()
     dom = max(range(16), key=lambda p: phase_ms[p])
     dom_ms = phase_ms[dom] / max(phase_cnt[dom], 1)
-    dom_bytes = phase_bytes(dom, n, n, nmat, phi, pml2)
+    dom_bytes = 8.0 * kd[dom]
     achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
-    step_bytes = sum(phase_bytes(p, n, n, nmat, phi, pml2) for p in range(16))
-    step_ms = ms / args.steps
+    step_ms = ms_max / args.steps
+    kernel_bytes_step = 8.0 * sum(kd.values())
+    manifest_bytes = 8.0 * manifest_doubles(nmat, run.damp_type, bool(run.porosity_model)) * cells
     breakdown = {PHASE_KERNELS[p]: round(phase_ms[p] / max(phase_cnt[p], 1), 4) for p in range(16) if phase_cnt[p]}
+    per_kernel = {PHASE_KERNELS[p]: {"ms": round(phase_ms[p] / phase_cnt[p], 4),
+                                     "bytes": 8.0 * kd[p],
+                                     "GBps": round(8.0 * kd[p] / (phase_ms[p] / phase_cnt[p] / 1000.0) / 1e9, 1),
+                                     "frac": round(8.0 * kd[p] / (phase_ms[p] / phase_cnt[p] / 1000.0) / 1e9 / hbm, 3)}
+                  for p in range(16) if phase_cnt[p] and kd[p] > 0}
 
     # end to end through the C ABI with host buffers: upload the initial state from pinned
     # host memory, K steps each reading back dt, time and the surface profile, then download
@@ -319,15 +385,20 @@ def run_gpu_arm(args):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "cells": cells, "materials": nmat, "form": "plain FP64",
                        "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "working set %.1f GB > 126 MB L2 (no flush needed)" % (step_bytes / 1e9),
-                       "init_s": round(init_s, 2)},
+                       "l2": "state %.1f GB, each step moves >= %.1f GB > 126 MB L2 (no flush needed)"
+                             % (h2d / 1e9, kernel_bytes_step / 1e9),
+                       "init_s": round(init_s, 2), "point_classes": counts, "tracers": ntr},
             "roofline": {"bound": "hbm", "kernel": PHASE_KERNELS[dom], "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": profile_traffic(PHASE_KERNELS[dom]), "bytes_per_launch": dom_bytes,
+                         "traffic": profile_traffic(PHASE_KERNELS[dom], cells), "bytes_per_launch": dom_bytes,
                          "launch_ms": dom_ms},
-            "step_roofline": {"algorithmic_bytes_per_cell_update": step_bytes / cells,
-                              "achieved_GBps": step_bytes / (step_ms / 1000.0) / 1e9,
-                              "frac": step_bytes / (step_ms / 1000.0) / 1e9 / hbm},
+            "step_roofline": {"manifest_bytes_per_cell_update": manifest_bytes / cells,
+                              "manifest_GBps": manifest_bytes / (step_ms / 1000.0) / 1e9,
+                              "manifest_frac": manifest_bytes / (step_ms / 1000.0) / 1e9 / hbm,
+                              "kernel_bytes_per_cell_update": kernel_bytes_step / cells,
+                              "kernel_GBps": kernel_bytes_step / (step_ms / 1000.0) / 1e9,
+                              "kernel_frac": kernel_bytes_step / (step_ms / 1000.0) / 1e9 / hbm},
+            "kernels": per_kernel,
             "kernel_ms": breakdown,
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": int(h2d / args.steps),
                     "d2h_bytes_per_step": int(d2h_step + d2h_out / args.steps)},
@@ -346,12 +417,12 @@ def run_gpu_arm(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=2048, help="cells per side of the GPU workload")
     ap.add_argument("--cpu-n", type=int, default=256, help="cells per side of the CPU sample")
-    ap.add_argument("--cpu-steps", type=int, default=60)
+    ap.add_argument("--cpu-steps", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 1:

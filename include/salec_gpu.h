@@ -135,8 +135,9 @@ int salec_gpu_get_field(salec_gpu *h, int field, double *host, long long n);
 /* Advance nsteps full cycles: the loop body of src/salec2d.c:115-272 without the output point. */
 int salec_gpu_step(salec_gpu *h, int nsteps);
 /* Run phases first..last of one cycle, for stepwise checks and timing. Phases follow the
- * reference's loop body (src/salec2d.c): 0 surface profile, 1 vertex volume fractions,
- * 2 vertex momentum + restriction, 3 cell velocity + ghosts, 4 void vertices, 5 velocity
+ * reference's loop body (src/salec2d.c): 0 surface profile, 1 vertex volume fractions and
+ * vertex momentum + restriction (one vertex sweep), 2 empty (the reference's second half of
+ * the vertex momentum update is done in 1), 3 cell velocity + ghosts, 4 void vertices, 5 velocity
  * gradient, viscosity and CFL candidates, 6 time step, 7 vibration/stress/damage, 8 vertex
  * acceleration (+ ghosts, restriction), 9 vertex displacement + restriction, 10 internal
  * energy, 11 tracers, 12 face fluxes (+ ghosts), 13 strength condition, 14 remap, damping,
@@ -165,6 +166,25 @@ int salec_gpu_get_tracers(salec_gpu *h, double *rows, int *n);
 
 /* Count non-finite values in the evolving cell and vertex fields; SALEC_ERR_NUMERIC if any. */
 int salec_gpu_check(salec_gpu *h, long long *n_bad);
+
+/*
+ * Output files of the current state, byte for byte those the reference writes for one rank
+ * (compiled with OUTPUT_GHT, as its CMakeLists does):
+ *   <dir>/vts/<prefix>.proc<rank>.<out_step>.vts          sale2d_write_vtk (src/write_vtk.c:189-298)
+ *   <dir>/vtp/<prefix>.tracer.proc<rank>.<out_step>.vtp   sale2d_write_vtp (src/write_vtk.c:354-480)
+ *   <dir>/txt/<prefix>.tracer.proc<rank>.<out_step>.txt   with SALEC_OUT_TRACER_TXT (:482-498)
+ * (rank and out_step printed %04d; out_step is the reference's k_out_step - 1). The reference
+ * writes in the middle of a cycle, after the flux and before the remap: run phases 0-13, call
+ * this, then phases 14-15. The device packs the arrays (FP64 -> FP32) and copies them to
+ * pinned host memory on the handle's stream; compression and file writing then run on host
+ * threads while the device continues. Without SALEC_OUT_WAIT the call returns once that work
+ * is queued; the next output call, salec_gpu_output_wait() or salec_gpu_destroy() waits for it
+ * and reports its errors.
+ */
+#define SALEC_OUT_WAIT 1
+#define SALEC_OUT_TRACER_TXT 2
+int salec_gpu_write_output(salec_gpu *h, const char *dir, const char *prefix, int rank, int out_step, int flags);
+int salec_gpu_output_wait(salec_gpu *h);
 
 /*
  * Boundary tables compiled to gather maps (host only, no device needed). The reference fills

@@ -46,16 +46,13 @@ GatherMap build_restrict_map(int vnx, int vny, int P, int ncomp, const int go[4]
 __global__ void k_profile_reset(const Ctx c);
 __global__ void k_trace_profile(const Ctx c);
 __global__ void k_profile_decode(const Ctx c);
-__global__ void k_vertex_vof(const Ctx c);
-__global__ void k_vertex_momentum(const Ctx c);
+__global__ void k_vertex_vof_momentum(const Ctx c);
 __global__ void k_cell_velocity(const Ctx c);
 __global__ void k_void_vertices(const Ctx c);
 __global__ void k_gradient_viscosity_cfl(const Ctx c);
 __global__ void k_finalize_dt(const Ctx c);
-__global__ void k_stress(const Ctx c);
 __global__ void k_vertex_acceleration(const Ctx c);
 __global__ void k_vertex_displacement(const Ctx c);
-__global__ void k_energy(const Ctx c);
 __global__ void k_tracers(const Ctx c);
 __global__ void k_cycle(const Ctx c);
 __global__ void k_record_reference_state(const Ctx c);
@@ -64,6 +61,8 @@ __global__ void k_gather(GatherBatch g, int mode, double *scratch);
 __global__ void k_aos_to_planes(const double *aos, double *base, long long plane, int P, int nx, int ny, int nc);
 __global__ void k_planes_to_aos(const double *base, double *aos, long long plane, int P, int nx, int ny, int nc);
 __global__ void k_count_nonfinite(const double *base, long long n, unsigned long long *out);
+void launch_stress(const Ctx &c, dim3 g, dim3 b, cudaStream_t s);
+void launch_energy(const Ctx &c, dim3 g, dim3 b, cudaStream_t s);
 void launch_flux(const Ctx &c, int pass, dim3 g, dim3 b, cudaStream_t s);
 void launch_remap_damp_state(const Ctx &c, int do_remap, int do_damp, int do_ejecta, int do_state, dim3 g, dim3 b,
                              cudaStream_t s);

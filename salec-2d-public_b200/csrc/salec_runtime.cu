@@ -94,6 +94,8 @@ struct Gather {
 
 } // namespace
 
+void salec_internal_output_release(void *&writer);   // salec_output.cu
+
 struct salec_gpu {
     Dims d{};
     RunParams rp{};
@@ -120,6 +122,7 @@ struct salec_gpu {
     std::vector<int> ev_phase;
     size_t ev_used = 0;
     long long launches = 0;     // kernels launched by this handle
+    void *output = nullptr;     // output writer state (salec_output.cu)
 
     Ctx ctx() const
     {
@@ -226,7 +229,7 @@ int run_phase(salec_gpu *h, int ph)
     const dim3 gc = grid2(h->d.enx, h->d.eny, blk), gv = grid2(h->d.vnx, h->d.vny, blk);
     cudaStream_t s = h->stream;
     int rc = SALEC_OK;
-    static const int kLaunches[16] = {3, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 2, 0, 1, 1};
+    static const int kLaunches[16] = {3, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1, 0, 2, 0, 1, 1};
     h->launches += kLaunches[ph] + (ph == 11 && h->tr.n > 0 ? 1 : 0);
     switch (ph) {
     case 0: {
@@ -236,15 +239,13 @@ int run_phase(salec_gpu *h, int ph)
         k_profile_decode<<<nb, 256, 0, s>>>(c);
         break;
     }
-    case 1:
+    case 1:   // vertex volume fractions and vertex momentum in one sweep (phase 2 is empty)
         rc = run_gather(h, h->g_mvof);
-        k_vertex_vof<<<gv, blk, 0, s>>>(c);
-        break;
-    case 2:
-        rc = run_gather(h, h->g_dvel_den);
-        k_vertex_momentum<<<gv, blk, 0, s>>>(c);
+        if (!rc) rc = run_gather(h, h->g_dvel_den);
+        k_vertex_vof_momentum<<<gv, blk, 0, s>>>(c);
         if (!rc) rc = run_gather(h, h->r_vel);
         break;
+    case 2: break;
     case 3:
         k_cell_velocity<<<gc, blk, 0, s>>>(c);
         rc = run_gather(h, h->g_evel);
@@ -252,7 +253,7 @@ int run_phase(salec_gpu *h, int ph)
     case 4: k_void_vertices<<<gv, blk, 0, s>>>(c); break;
     case 5: k_gradient_viscosity_cfl<<<gc, blk, 0, s>>>(c); break;
     case 6: k_finalize_dt<<<1, 32, 0, s>>>(c); break;
-    case 7: k_stress<<<gc, blk, 0, s>>>(c); break;
+    case 7: launch_stress(c, gc, blk, s); break;
     case 8:
         rc = run_gather(h, h->g_pre_ste_q);
         k_vertex_acceleration<<<gv, blk, 0, s>>>(c);
@@ -262,7 +263,7 @@ int run_phase(salec_gpu *h, int ph)
         k_vertex_displacement<<<gv, blk, 0, s>>>(c);
         rc = run_gather(h, h->r_dis);
         break;
-    case 10: k_energy<<<gc, blk, 0, s>>>(c); break;
+    case 10: launch_energy(c, gc, blk, s); break;
     case 11:
         if (h->tr.n > 0) k_tracers<<<(h->tr.n + 127) / 128, 128, 0, s>>>(c);
         break;
@@ -399,6 +400,7 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
 void release(salec_gpu *h)
 {
     if (!h) return;
+    salec_internal_output_release(h->output);
     for (void *p : h->owned) cudaFree(p);
     if (h->pool) cudaFree(h->pool);
     if (h->staging) cudaFree(h->staging);
@@ -446,6 +448,25 @@ int salec_internal_finish_init(salec_gpu *h, double damp_time_in, double *damp_t
 }
 
 int salec_internal_fail(int code, const char *msg) { return fail(code, msg ? msg : "error"); }
+
+// Views of the handle for the output writer (salec_output.cu).
+int salec_internal_field_view(salec_gpu *h, const char *name, const double **base, long long *plane, int *pitch,
+                              int *nx, int *ny, int *nc)
+{
+    const int fid = field_by_name(name);
+    if (fid < 0) return fail(SALEC_ERR_ARG, std::string("unknown field ") + name);
+    field_points(h, fid, *nx, *ny);
+    *nc = field_ncomp(h, fid);
+    *base = field_ptr(h, fid);
+    *plane = kFields[fid].loc == L_COL ? 0 : h->d.PL;
+    *pitch = h->d.P;
+    return SALEC_OK;
+}
+cudaStream_t salec_internal_stream(salec_gpu *h) { return h->stream; }
+Tracers salec_internal_tracers(salec_gpu *h) { return h->tr; }
+Dims salec_internal_dims(salec_gpu *h) { return h->d; }
+void salec_internal_add_launches(salec_gpu *h, int n) { h->launches += n; }
+void *&salec_internal_output_slot(salec_gpu *h) { return h->output; }
 
 // ================================================================== C ABI
 extern "C" {

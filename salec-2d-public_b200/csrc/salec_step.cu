@@ -81,10 +81,8 @@ __global__ void k_profile_decode(const Ctx c)
 
 // ============================================================ phase 1: vertex volume fractions
 // update_v_vof (src/sale2d.c:751-791): mean of the four surrounding cells.
-__global__ void k_vertex_vof(const Ctx c)
+__device__ __forceinline__ void vertex_vof(const Ctx &c, int i, int j)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (!vert_active(c, i, j)) return;
     const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
     const long long p = KIDX(i, j);
     for (int m = 0; m < c.d.nmat; ++m) {
@@ -98,10 +96,8 @@ __global__ void k_vertex_vof(const Ctx c)
 // ============================================================ phase 2: vertex momentum
 // update_v_vel_inc (src/sale2d.c:930-1049): add the advected momentum increments of the
 // four cells, weighted by density and corner sub-volume; clamp |v|; count void corners.
-__global__ void k_vertex_momentum(const Ctx c)
+__device__ __forceinline__ void vertex_momentum(const Ctx &c, int i, int j)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (!vert_active(c, i, j)) return;
     const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
     const int corner[4] = {2, 3, 0, 1};
     const long long p = KIDX(i, j);
@@ -142,6 +138,16 @@ __global__ void k_vertex_momentum(const Ctx c)
     }
     if (vn < c.rp.velocity_min * 1) { nx_ = 0.; ny_ = 0.; }
     vx[p] = nx_; vy[p] = ny_;
+}
+
+// Phases 1 and 2 in one vertex sweep: both read only cell fields that no vertex sweep writes,
+// so one thread per vertex does both (the m_vof and e_dvel/e_den ghost fills run first).
+__global__ void k_vertex_vof_momentum(const Ctx c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!vert_active(c, i, j)) return;
+    vertex_vof(c, i, j);
+    vertex_momentum(c, i, j);
 }
 
 // ============================================================ phase 3: cell velocity
@@ -284,12 +290,14 @@ __global__ void k_finalize_dt(const Ctx c)
 
 // ============================================================ phase 7: vibration, stress, damage
 // block_vibration (src/strength.c:625-695) and update_e_stress (src/strength.c:7-349).
-__global__ void k_stress(const Ctx c)
+template <int NM, bool POR>
+__global__ void __launch_bounds__(256) k_stress(const Ctx c)
 {
+    constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!cell_interior(c, i, j)) return;
     const long long p = KIDX(i, j);
-    const int nmat = c.d.nmat;
+    const int nmat = NM > 0 ? NM : c.d.nmat;
     const double dt = c.scal->dt;
     const double vof0 = c.f.m_vof[p];
     double dam = c.f.e_dam[p];
@@ -330,27 +338,41 @@ __global__ void k_stress(const Ctx c)
     }
 
     // --- stress update
-    double s0 = c.f.e_ste[p], s1 = PLN(c.f.e_ste, 1)[p], s2 = PLN(c.f.e_ste, 2)[p], s3 = PLN(c.f.e_ste, 3)[p];
-    double ste2s = c.f.e_ste2s[p], sta2s = c.f.e_sta2s[p], tps = c.f.e_tps[p], strength = c.f.e_strength[p];
     if (vof0 > SALEC_TOLVOF) {
         c.f.e_ste[p] = 0.; PLN(c.f.e_ste, 1)[p] = 0.; PLN(c.f.e_ste, 2)[p] = 0.; PLN(c.f.e_ste, 3)[p] = 0.;
         c.f.e_ste2s[p] = 0.; c.f.e_sta2s[p] = 0.; c.f.e_strength[p] = 0.;
         return;
     }
-    double vapor_ref = 0., melt_ref = 0.;
+    // every input of a full cell, issued in one batch
+    double s0 = c.f.e_ste[p], s1 = PLN(c.f.e_ste, 1)[p], s2 = PLN(c.f.e_ste, 2)[p], s3 = PLN(c.f.e_ste, 3)[p];
+    double ste2s = c.f.e_ste2s[p], sta2s = c.f.e_sta2s[p], tps = c.f.e_tps[p], strength = c.f.e_strength[p];
+    double vmat[MM], ptm[MM];
+    #pragma unroll
     for (int m = 1; m < nmat; ++m) {
-        const double vm = PLN(c.f.m_vof, m)[p];
+        vmat[m] = PLN(c.f.m_vof, m)[p];
+        ptm[m] = POR ? PLN(c.f.m_pty, m)[p] : 1.0;
+    }
+    const double rho = c.f.e_den[p];
+    const double g0 = c.f.e_grad_vel[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
+                 g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
+    const double mu = c.f.e_mu[p];
+    const double pre = c.f.e_pre[p], tem = c.f.e_tem[p], csd = c.f.e_csd[p];
+    double vapor_ref = 0., melt_ref = 0.;
+    #pragma unroll
+    for (int m = 1; m < nmat; ++m) {
+        const double vm = vmat[m];
         if (vm < SALEC_TOLVOF) continue;
         vapor_ref += vm * c.mat[m].VaporDen;
         melt_ref += vm * c.mat[m].MeltDen;
     }
     double porosity = 0.0;
-    if (c.rp.porosity_model) {
+    if (POR) {
         double mv = 0.0;
+        #pragma unroll
         for (int m = 1; m < nmat; ++m) {
-            const double vm = PLN(c.f.m_vof, m)[p];
+            const double vm = vmat[m];
             if (vm < SALEC_TOLVOF) continue;
-            porosity += vm * PLN(c.f.m_pty, m)[p];
+            porosity += vm * ptm[m];
             mv += vm;
         }
         porosity /= mv;
@@ -361,11 +383,8 @@ __global__ void k_stress(const Ctx c)
     vapor_ref /= porosity;
     melt_ref /= porosity;
 
-    const double rho = c.f.e_den[p];
     const double ste2s_old = ste2s;
     int state; // 0 solid, 1 melt, 2 vapour
-    const double g0 = c.f.e_grad_vel[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
-                 g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
     if (rho <= vapor_ref) {
         state = 2;
         s0 = s1 = s2 = s3 = 0.;
@@ -398,7 +417,7 @@ __global__ void k_stress(const Ctx c)
             const double r1 = s1 * cos2o1 - ss2 * sin2o;
             const double r2 = -ss2 * cos2o1 - s1 * sin2o;
             s0 += 1.0 * r0; s1 += 1.0 * r1; s2 += 1.0 * r2; s3 += 1.0 * 0.0;
-            const double k2 = 2.0 * c.f.e_mu[p] * dt;
+            const double k2 = 2.0 * mu * dt;
             s0 += k2 * e0; s1 += k2 * e1; s2 += k2 * e2; s3 += k2 * e3;
             ste2s = sqrt(second_inv(s0, s1, s2, s3));
             sta2s = sqrt(second_inv(e0, e1, e2, e3));
@@ -410,15 +429,15 @@ __global__ void k_stress(const Ctx c)
     } else if (state == 1) {
         dam = 1.0;
     } else {
-        const double pre = c.f.e_pre[p], tem = c.f.e_tem[p];
         double shear = 0.0, tensile = 0.;
+        #pragma unroll
         for (int m = 1; m < nmat; ++m) {
-            const double vm = PLN(c.f.m_vof, m)[p];
+            const double vm = vmat[m];
             if (vm < SALEC_TOLVOF) continue;
             const DevMat &s = c.mat[m];
             double my = strength_fn(s.yfunc, pre, dam, tps, sta2s, tem, 0., s);
             if (c.rp.acoustic_fluid && pre >= 0.) {
-                const double vibp = dmin(rho * c.f.e_csd[p] * sqrt(c.f.e_vib[p]), pre);
+                const double vibp = dmin(rho * csd * sqrt(c.f.e_vib[p]), pre);
                 const double tm = simon_melt(pre, s);
                 double soft = ohnaka_soft(tem, s, tm);
                 soft = wind(soft, 0.0, 1.0);
@@ -440,9 +459,10 @@ __global__ void k_stress(const Ctx c)
             s0 *= sfac; s1 *= sfac; s2 *= sfac; s3 *= sfac;
             ste2s = shear;
             double dsd = 0.;
+            #pragma unroll
             for (int m = 1; m < nmat; ++m) {
                 const DevMat &s = c.mat[m];
-                dsd += PLN(c.f.m_vof, m)[p] * strength_fn(s.dsdf, pre, dam, 0., 0., 0., 0., s);
+                dsd += vmat[m] * strength_fn(s.dsdf, pre, dam, 0., 0., 0., 0., s);
             }
             dam = wind(dam + sta2s * dsd * dt, 0.0, 1.0);
             tps = dmin(tps + sta2s * dt, 10.);
@@ -454,7 +474,7 @@ __global__ void k_stress(const Ctx c)
             tmax = dmax(tmax, sth);
             if ((tmax - pre) > tensile) {
                 // the reference divides by Min(e_pos[1], e_pos[2]) (centre y and scale x)
-                const double dinc = 0.4 * c.f.e_csd[p] / dmin(PLN(c.f.e_pos, 1)[p], PLN(c.f.e_pos, 2)[p]);
+                const double dinc = 0.4 * csd / dmin(PLN(c.f.e_pos, 1)[p], PLN(c.f.e_pos, 2)[p]);
                 const double dold = dam;
                 double third = pow(dold, 1.0 / 3.);
                 third += dinc;
@@ -591,54 +611,68 @@ __global__ void k_vertex_displacement(const Ctx c)
 }
 
 // ============================================================ phase 10: internal energy
-// update_energy (src/sale2d.c:564-712) with the Wunnemann porosity update.
-__global__ void k_energy(const Ctx c)
+// update_energy (src/sale2d.c:564-712) with the Wunnemann porosity update. After the vacuum
+// test, every input of the cell is loaded in one batch (no load waits on another).
+template <int NM, bool POR>
+__global__ void __launch_bounds__(256) k_energy(const Ctx c)
 {
+    constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!cell_interior(c, i, j)) return;
     const long long p = KIDX(i, j);
-    const int nmat = c.d.nmat;
+    const int nmat = NM > 0 ? NM : c.d.nmat;
     if (c.f.m_vof[p] > SALEC_TOLVOF || c.f.e_den[p] < SALEC_TOLRHO) return;
+    double vm[MM], rm[MM], em[MM], pt[MM];
+    #pragma unroll
+    for (int m = 1; m < nmat; ++m) {
+        vm[m] = PLN(c.f.m_vof, m)[p];
+        rm[m] = PLN(c.f.m_den, m)[p];
+        em[m] = PLN(c.f.m_eng, m)[p];
+        pt[m] = POR ? PLN(c.f.m_pty, m)[p] : 1.0;
+    }
     const double dt = c.scal->dt;
     const double pre = c.f.e_pre[p];
-    const double lp = pre + c.f.e_q[p];
+    const double q = c.f.e_q[p];
     const double div = c.f.e_div_vel[p];
-    const double dE_pre = -lp * div;
     const double g0 = c.f.e_grad_vel[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
                  g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
-    const double dE_ste = c.f.e_ste[p] * g0 + PLN(c.f.e_ste, 1)[p] * (g1 + g2) + PLN(c.f.e_ste, 2)[p] * g3
-                        + PLN(c.f.e_ste, 3)[p] * g4;
-    double gam = 0.;
-    for (int m = 1; m < nmat; ++m) {
-        const double vm = PLN(c.f.m_vof, m)[p];
-        if (vm > SALEC_TOLVOF) gam += vm * c.mat[m].gamfrac / PLN(c.f.m_den, m)[p];
+    const double s0 = c.f.e_ste[p], s1 = PLN(c.f.e_ste, 1)[p], s2 = PLN(c.f.e_ste, 2)[p], s3 = PLN(c.f.e_ste, 3)[p];
+    const double cvs_old = c.f.e_cvs[p];
+    double sig = 0., ev0 = 0., ev1 = 0.;
+    if (POR) {
+        sig = c.f.e_sigma[p] + PLN(c.f.e_sigma, 1)[p];
+        ev0 = c.f.e_vel[p];
+        ev1 = PLN(c.f.e_vel, 1)[p];
     }
+    const double lp = pre + q;
+    const double dE_pre = -lp * div;
+    const double dE_ste = s0 * g0 + s1 * (g1 + g2) + s2 * g3 + s3 * g4;
+    double gam = 0.;
+    #pragma unroll
+    for (int m = 1; m < nmat; ++m)
+        if (vm[m] > SALEC_TOLVOF) gam += vm[m] * c.mat[m].gamfrac / rm[m];
     const double dcvs = div - gam * (dE_pre + dE_ste);
-    const double cvs = c.rp.porosity_model ? c.f.e_cvs[p] : 0.0;
+    const double cvs = POR ? cvs_old : 0.0;
+    #pragma unroll
     for (int m = 1; m < nmat; ++m) {
-        const double vm = PLN(c.f.m_vof, m)[p];
-        const double rm = PLN(c.f.m_den, m)[p];
-        double *em = PLN(c.f.m_eng, m) + p;
-        if (vm <= SALEC_TOLVOF || rm <= SALEC_TOLRHO) {
-            *em = 0.;
-            if (c.rp.porosity_model) PLN(c.f.m_pty, m)[p] = 1.;
+        if (vm[m] <= SALEC_TOLVOF || rm[m] <= SALEC_TOLRHO) {
+            em[m] = 0.;
+            if (POR) pt[m] = 1.;
         } else {
             const double fac = 1.0;
-            *em = dmax(0., *em + (dE_pre + dE_ste) * dt * fac);
-            if (c.rp.porosity_model) {
-                double *pt = PLN(c.f.m_pty, m) + p;
+            em[m] = dmax(0., em[m] + (dE_pre + dE_ste) * dt * fac);
+            if (POR) {
                 double dpty = 0.;
-                if (c.f.e_sigma[p] + PLN(c.f.e_sigma, 1)[p] <= 0.) {
-                    dpty = strength_fn(c.mat[m].porfunc, *pt, cvs, pre, dcvs, c.f.e_vel[p], PLN(c.f.e_vel, 1)[p],
-                                       c.mat[m]);
-                }
-                *pt += dpty * dt;
-                *pt = wind(*pt, 1.0, c.mat[m].alphamax2);
+                if (sig <= 0.) dpty = strength_fn(c.mat[m].porfunc, pt[m], cvs, pre, dcvs, ev0, ev1, c.mat[m]);
+                pt[m] += dpty * dt;
+                pt[m] = wind(pt[m], 1.0, c.mat[m].alphamax2);
             }
         }
+        PLN(c.f.m_eng, m)[p] = em[m];
+        if (POR) PLN(c.f.m_pty, m)[p] = pt[m];
     }
     // the reference updates e_cvs for every non-vacuum cell, with or without porosity
-    c.f.e_cvs[p] = wind(c.f.e_cvs[p] + dcvs * dt, -10.0, 10.0);
+    c.f.e_cvs[p] = wind(cvs_old + dcvs * dt, -10.0, 10.0);
 }
 
 // ============================================================ phase 11: tracers
@@ -862,7 +896,6 @@ __global__ void __launch_bounds__(256) k_flux(const Ctx c, int pass)
     const double bv = swept_volume(px[1], py[1], px[0], py[0], dx[1], dy[1], dx[0], dy[0]);
     const double uv = swept_volume(px[3], py[3], px[2], py[2], dx[3], dy[3], dx[2], dy[2]);
     const double lbru[4] = {lv, bv, rv, uv};
-
     double vof[MM];
     #pragma unroll
     for (int m = 0; m < nmat; ++m) vof[m] = PLN(c.f.m_vof, m)[p];
@@ -1019,10 +1052,68 @@ __global__ void __launch_bounds__(256) k_flux(const Ctx c, int pass)
 // advect_flux_default (src/advect.c:26-302), damp_on_cell (src/velocity.c:356-767),
 // ejecta_flow (src/ejecta.c:65-133) and update_state (src/sale2d.c:1635-1742), fused per cell:
 // the damping reads only its own cell, and the EOS reads the damped material state.
+// The cell's state travels through remap, damping, ejecta drag and EOS in registers: each
+// member is loaded once and stored once per step.
 template <int NM, bool POR>
-__device__ __forceinline__ void remap_cell(const Ctx &c, int i, int j, long long p)
+struct CellState {
+    static constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
+    double vof[MM], rho[MM], eng[MM], pty[MM];
+    double dvx, dvy, st[4], dam, tps, vib, ejt, cvs, eden;
+};
+
+template <int NM, bool POR>
+__device__ __forceinline__ void load_cell(const Ctx &c, long long p, CellState<NM, POR> &s)
 {
-    constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
+    const int nmat = NM > 0 ? NM : c.d.nmat;
+    #pragma unroll
+    for (int m = 0; m < nmat; ++m) {
+        s.vof[m] = PLN(c.f.m_vof, m)[p];
+        s.rho[m] = PLN(c.f.m_den, m)[p];
+        s.eng[m] = PLN(c.f.m_eng, m)[p];
+        s.pty[m] = POR ? PLN(c.f.m_pty, m)[p] : 1.0;
+    }
+    s.dvx = c.f.e_dvel[p];
+    s.dvy = PLN(c.f.e_dvel, 1)[p];
+    #pragma unroll
+    for (int q = 0; q < 4; ++q) s.st[q] = PLN(c.f.e_ste, q)[p];
+    s.dam = c.f.e_dam[p];
+    s.tps = c.f.e_tps[p];
+    s.vib = c.f.e_vib[p];
+    s.ejt = c.f.e_ejt[p];
+    s.cvs = POR ? c.f.e_cvs[p] : 0.0;
+    s.eden = c.f.e_den[p];
+}
+
+template <int NM, bool POR>
+__device__ __forceinline__ void store_cell(const Ctx &c, long long p, const CellState<NM, POR> &s, bool den)
+{
+    const int nmat = NM > 0 ? NM : c.d.nmat;
+    #pragma unroll
+    for (int m = 0; m < nmat; ++m) {
+        PLN(c.f.m_vof, m)[p] = s.vof[m];
+        PLN(c.f.m_den, m)[p] = s.rho[m];
+        PLN(c.f.m_eng, m)[p] = s.eng[m];
+        if (POR) PLN(c.f.m_pty, m)[p] = s.pty[m];
+    }
+    c.f.e_dvel[p] = s.dvx;
+    PLN(c.f.e_dvel, 1)[p] = s.dvy;
+    #pragma unroll
+    for (int q = 0; q < 4; ++q) PLN(c.f.e_ste, q)[p] = s.st[q];
+    c.f.e_dam[p] = s.dam;
+    c.f.e_tps[p] = s.tps;
+    c.f.e_vib[p] = s.vib;
+    c.f.e_ejt[p] = s.ejt;
+    if (POR) c.f.e_cvs[p] = s.cvs;
+    if (den) c.f.e_den[p] = s.eden;
+}
+
+// advect_flux_default (src/advect.c:26-302) for one interior cell, into registers. The loads
+// that do not depend on the flow (the cell's own state and the material volumes of its four
+// faces) are all issued before the first dependent one.
+template <int NM, bool POR>
+__device__ __forceinline__ void remap_cell(const Ctx &c, int i, int j, long long p, CellState<NM, POR> &s)
+{
+    constexpr int MM = CellState<NM, POR>::MM;
     const int nmat = NM > 0 ? NM : c.d.nmat;
     const int phi = 3 * nmat + 10 + (POR ? nmat + 1 : 0);
     const long long PL = c.d.PL;
@@ -1030,15 +1121,37 @@ __device__ __forceinline__ void remap_cell(const Ctx &c, int i, int j, long long
     const double *face[4] = {c.f.bx_phi + KIDX(i, j), c.f.by_phi + KIDX(i, j), c.f.bx_phi + KIDX(i + 1, j),
                              c.f.by_phi + KIDX(i, j + 1)};
     const double dir[4] = {1.0, 1.0, -1.0, -1.0};
+    double fv[4][MM];
+    #pragma unroll
+    for (int k = 0; k < 4; ++k)
+        #pragma unroll
+        for (int m = 0; m < nmat; ++m) fv[k][m] = face[k][m * PL];
+    double vof[MM], rho[MM], eng[MM], pty[MM];
+    #pragma unroll
+    for (int m = 0; m < nmat; ++m) {
+        vof[m] = PLN(c.f.m_vof, m)[p];
+        rho[m] = PLN(c.f.m_den, m)[p];
+        eng[m] = PLN(c.f.m_eng, m)[p];
+        pty[m] = por ? PLN(c.f.m_pty, m)[p] : 1.0;
+    }
+    const double evol = c.f.e_vol[p];
+    const double eden0 = c.f.e_den[p];
+    double st0[4];
+    #pragma unroll
+    for (int q = 0; q < 4; ++q) st0[q] = PLN(c.f.e_ste, q)[p];
+    const double dam0 = c.f.e_dam[p], tps0 = c.f.e_tps[p], vib0 = c.f.e_vib[p], ejt0 = c.f.e_ejt[p];
+    const double cvs0 = por ? c.f.e_cvs[p] : 0.0;
+
     double dphi[4 * MM + 11];
     #pragma unroll
     for (int q = 0; q < phi; ++q) dphi[q] = 0.;
     const int b = 3 * nmat;
+    #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const double *f = face[k];
         #pragma unroll
         for (int m = 0; m < nmat; ++m) {
-            const double mv = dir[k] * f[m * PL];
+            const double mv = dir[k] * fv[k][m];
             if (mv == 0.0) continue;   // adds only signed zeros to dphi (see k_flux)
             const double rho_f = f[(m + nmat) * PL];
             dphi[m] += mv;
@@ -1053,38 +1166,29 @@ __device__ __forceinline__ void remap_cell(const Ctx &c, int i, int j, long long
             }
         }
     }
-    double vof[MM], rho[MM], eng[MM], pty[MM];
+    // sphi = cell content + face fluxes, accumulated in place in dphi (the content of each
+    // member is formed as 0 + term, then the flux sum is added, as in the reference)
+    double emass = evol * eden0;
+    double *sphi = dphi;
     #pragma unroll
     for (int m = 0; m < nmat; ++m) {
-        vof[m] = PLN(c.f.m_vof, m)[p];
-        rho[m] = PLN(c.f.m_den, m)[p];
-        eng[m] = PLN(c.f.m_eng, m)[p];
-        pty[m] = por ? PLN(c.f.m_pty, m)[p] : 1.0;
+        sphi[m] = (0.0 + vof[m] * evol) + 1.0 * dphi[m];
+        sphi[m + nmat] = (0.0 + vof[m] * evol * rho[m]) + 1.0 * dphi[m + nmat];
+        sphi[m + 2 * nmat] = (0.0 + vof[m] * evol * eng[m]) + 1.0 * dphi[m + 2 * nmat];
     }
-    const double evol = c.f.e_vol[p];
-    double emass = evol * c.f.e_den[p];
-    double sphi[4 * MM + 11];
+    sphi[b] = 0.0 + 1.0 * dphi[b];
+    sphi[b + 1] = 0.0 + 1.0 * dphi[b + 1];
     #pragma unroll
-    for (int q = 0; q < phi; ++q) sphi[q] = 0.;
-    #pragma unroll
-    for (int m = 0; m < nmat; ++m) {
-        sphi[m] += vof[m] * evol;
-        sphi[m + nmat] += vof[m] * evol * rho[m];
-        sphi[m + 2 * nmat] += vof[m] * evol * eng[m];
-    }
-    #pragma unroll
-    for (int q = 0; q < 4; ++q) sphi[b + 2 + q] += emass * PLN(c.f.e_ste, q)[p];
-    sphi[b + 6] = emass * c.f.e_dam[p];
-    sphi[b + 7] = emass * c.f.e_tps[p];
-    sphi[b + 8] = emass * c.f.e_vib[p];
-    sphi[b + 9] = emass * c.f.e_ejt[p];
+    for (int q = 0; q < 4; ++q) sphi[b + 2 + q] = (0.0 + emass * st0[q]) + 1.0 * dphi[b + 2 + q];
+    sphi[b + 6] = emass * dam0 + 1.0 * dphi[b + 6];
+    sphi[b + 7] = emass * tps0 + 1.0 * dphi[b + 7];
+    sphi[b + 8] = emass * vib0 + 1.0 * dphi[b + 8];
+    sphi[b + 9] = emass * ejt0 + 1.0 * dphi[b + 9];
     if (por) {
-        sphi[b + 10] = emass * c.f.e_cvs[p];
+        sphi[b + 10] = emass * cvs0 + 1.0 * dphi[b + 10];
         #pragma unroll
-        for (int m = 0; m < nmat; ++m) sphi[b + 11 + m] = vof[m] * evol * rho[m] * pty[m];
+        for (int m = 0; m < nmat; ++m) sphi[b + 11 + m] = vof[m] * evol * rho[m] * pty[m] + 1.0 * dphi[b + 11 + m];
     }
-    #pragma unroll
-    for (int q = 0; q < phi; ++q) sphi[q] += 1.0 * dphi[q];
     double zeta = 0.0;
     emass = 0.;
     #pragma unroll
@@ -1095,23 +1199,23 @@ __device__ __forceinline__ void remap_cell(const Ctx &c, int i, int j, long long
         emass += sphi[m + nmat];
     }
     if (zeta > evol * (1.0 - SALEC_TOLVOF) || (zeta > 0. && sphi[0] < evol * SALEC_TOLVOF)) {
-        const double s = 1.0 / zeta;
+        const double sc = 1.0 / zeta;
         #pragma unroll
-        for (int m = 0; m < nmat; ++m) vof[m] = s * sphi[m];
+        for (int m = 0; m < nmat; ++m) vof[m] = sc * sphi[m];
         vof[0] = 0.0;
     } else if (zeta < evol * SALEC_TOLVOF) {
         #pragma unroll
         for (int m = 0; m < nmat; ++m) vof[m] = 0.;
         vof[0] = 1.0;
     } else if (c.rp.partpres) {
-        const double s = 1.0 / (zeta + sphi[0]);
+        const double sc = 1.0 / (zeta + sphi[0]);
         #pragma unroll
-        for (int m = 0; m < nmat; ++m) vof[m] = s * sphi[m];
+        for (int m = 0; m < nmat; ++m) vof[m] = sc * sphi[m];
     } else {
         sphi[0] = evol - zeta;
-        const double s = 1.0 / evol;
+        const double sc = 1.0 / evol;
         #pragma unroll
-        for (int m = 0; m < nmat; ++m) vof[m] = s * sphi[m];
+        for (int m = 0; m < nmat; ++m) vof[m] = sc * sphi[m];
     }
     #pragma unroll
     for (int m = 1; m < nmat; ++m) {
@@ -1124,12 +1228,12 @@ __device__ __forceinline__ void remap_cell(const Ctx &c, int i, int j, long long
             if (por) pty[m] = sphi[b + 11 + m] / sphi[m + nmat];
         }
     }
-    double dvx, dvy, st[4], dam, tps, vib, ejt, cvs = por ? c.f.e_cvs[p] : 0.0;
+    double dvx, dvy, st[4], dam, tps, vib, ejt, cvs = cvs0;
     if (emass > SALEC_TOLRHO * evol) {
-        const double s = 1.0 / emass;
-        dvx = s * sphi[b]; dvy = s * sphi[b + 1];
+        const double sc = 1.0 / emass;
+        dvx = sc * sphi[b]; dvy = sc * sphi[b + 1];
         #pragma unroll
-        for (int q = 0; q < 4; ++q) st[q] = s * sphi[b + 2 + q];
+        for (int q = 0; q < 4; ++q) st[q] = sc * sphi[b + 2 + q];
         dam = sphi[b + 6] / emass;
         tps = sphi[b + 7] / emass;
         vib = sphi[b + 8] / emass;
@@ -1162,31 +1266,37 @@ __device__ __forceinline__ void remap_cell(const Ctx &c, int i, int j, long long
         }
     }
     #pragma unroll
-    for (int m = 0; m < nmat; ++m) {
-        PLN(c.f.m_vof, m)[p] = vof[m];
-        PLN(c.f.m_den, m)[p] = rho[m];
-        PLN(c.f.m_eng, m)[p] = eng[m];
-        if (por) PLN(c.f.m_pty, m)[p] = pty[m];
-    }
-    c.f.e_dvel[p] = dvx;
-    PLN(c.f.e_dvel, 1)[p] = dvy;
+    for (int m = 0; m < nmat; ++m) { s.vof[m] = vof[m]; s.rho[m] = rho[m]; s.eng[m] = eng[m]; s.pty[m] = pty[m]; }
+    s.dvx = dvx; s.dvy = dvy;
     #pragma unroll
-    for (int q = 0; q < 4; ++q) PLN(c.f.e_ste, q)[p] = st[q];
-    c.f.e_dam[p] = dam;
-    c.f.e_tps[p] = tps;
-    c.f.e_vib[p] = vib;
-    c.f.e_ejt[p] = ejt;
-    if (por) c.f.e_cvs[p] = cvs;
-    c.f.e_den[p] = eden;
+    for (int q = 0; q < 4; ++q) s.st[q] = st[q];
+    s.dam = dam; s.tps = tps; s.vib = vib; s.ejt = ejt; s.cvs = cvs; s.eden = eden;
 }
 
+// The lowest material index whose volume fraction is at least (strict: above) 1 - TOLVOF, or
+// -1: the material the damping of a full cell acts on.
 template <int NM, bool POR>
-__device__ __forceinline__ void damp_cell(const Ctx &c, long long p, double dt)
+__device__ __forceinline__ int first_material(const CellState<NM, POR> &s, int nmat, bool strict)
+{
+    int mf = -1;
+    #pragma unroll
+    for (int m = (NM > 0 ? NM : SALEC_MAXMAT) - 1; m >= 1; --m) {
+        if (m >= nmat) continue;
+        const bool full = strict ? s.vof[m] > 1.0 - SALEC_TOLVOF : s.vof[m] >= 1.0 - SALEC_TOLVOF;
+        if (full) mf = m;
+    }
+    return mf;
+}
+
+// damp_on_cell (src/velocity.c:356-767) on the register state; the auxiliary e_alpha is read
+// and written here. Returns whether the cell's state changed.
+template <int NM, bool POR>
+__device__ __forceinline__ bool damp_cell(const Ctx &c, long long p, double dt, CellState<NM, POR> &s)
 {
     const int nmat = NM > 0 ? NM : c.d.nmat;
     const int ty = c.rp.damp_type;
-    if (ty == 4 || ty == 5) return;
-    if (c.f.m_vof[p] > SALEC_TOLVOF) return;
+    if (ty == 4 || ty == 5) return false;
+    if (s.vof[0] > SALEC_TOLVOF) return false;
     const double sx = c.f.e_sigma[p], sy = PLN(c.f.e_sigma, 1)[p];
     const double d0 = c.f.e_dampref[p], d1 = PLN(c.f.e_dampref, 1)[p];
     constexpr bool por = POR;
@@ -1196,143 +1306,147 @@ __device__ __forceinline__ void damp_cell(const Ctx &c, long long p, double dt)
         const double pre = c.f.e_pre[p];
         if (sy > 0.0) {
             ay += (sy * PLN(c.f.e_grad_vel, 0)[p] + sy * PLN(c.f.e_grad_vel, 4)[p] - c.rp.alpha_damp_y * ay) * dt;
-            PLN(c.f.e_dvel, 1)[p] += -1.0 * sy * PLN(c.f.e_vel, 1)[p] * dt;
+            s.dvy += -1.0 * sy * PLN(c.f.e_vel, 1)[p] * dt;
+            const int mf = first_material(s, nmat, false);
             #pragma unroll
             for (int m = 1; m < nmat; ++m) {
-                if (PLN(c.f.m_vof, m)[p] < 1.0 - SALEC_TOLVOF) continue;
-                double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
-                const double pt = por ? PLN(c.f.m_pty, m)[p] : 1.0;
-                const double rd = (-sy * (*rm - d0) - d0 * ay) * dt;
-                const double ed = (-sy * (*em - d1) - pre * ay) * dt;
-                *rm += rd / pt;
-                *em += ed / pt;
-                break;
+                if (m != mf) continue;
+                const double pt = por ? s.pty[m] : 1.0;
+                const double rd = (-sy * (s.rho[m] - d0) - d0 * ay) * dt;
+                const double ed = (-sy * (s.eng[m] - d1) - pre * ay) * dt;
+                s.rho[m] += rd / pt;
+                s.eng[m] += ed / pt;
             }
         }
         if (sx > 0.0) {
             ax += (sx * PLN(c.f.e_grad_vel, 3)[p] + sx * PLN(c.f.e_grad_vel, 4)[p] - c.rp.alpha_damp_x * ax) * dt;
-            c.f.e_dvel[p] += -1.0 * sx * c.f.e_vel[p] * dt;
+            s.dvx += -1.0 * sx * c.f.e_vel[p] * dt;
+            const int mf = first_material(s, nmat, true);
             #pragma unroll
             for (int m = 1; m < nmat; ++m) {
-                if (PLN(c.f.m_vof, m)[p] > 1.0 - SALEC_TOLVOF) {
-                    double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
-                    const double pt = por ? PLN(c.f.m_pty, m)[p] : 1.0;
-                    const double rd = (-sx * (*rm - d0) - d0 * (ax + ay)) * dt;
-                    const double ed = (-sx * (*em - d1) - pre * (ax + ay)) * dt;
-                    *rm += rd / pt;
-                    *em += ed / pt;
-                    break;
-                }
+                if (m != mf) continue;
+                const double pt = por ? s.pty[m] : 1.0;
+                const double rd = (-sx * (s.rho[m] - d0) - d0 * (ax + ay)) * dt;
+                const double ed = (-sx * (s.eng[m] - d1) - pre * (ax + ay)) * dt;
+                s.rho[m] += rd / pt;
+                s.eng[m] += ed / pt;
             }
         }
         c.f.e_alpha[p] = ax;
         PLN(c.f.e_alpha, 1)[p] = ay;
+        return sx > 0.0 || sy > 0.0;
     } else if (ty == 1 || ty == 2) {
         // damp_on_cell_pml2 / _pml3 (src/velocity.c:471-654)
-        if (!(sy > 0.0 || sx > 0.0)) return;
+        if (!(sy > 0.0 || sx > 0.0)) return false;
         const double ss = sx + sy;
-        c.f.e_dvel[p] += -1.0 * ss * c.f.e_vel[p] * dt;
-        PLN(c.f.e_dvel, 1)[p] += -1.0 * ss * PLN(c.f.e_vel, 1)[p] * dt;
+        s.dvx += -1.0 * ss * c.f.e_vel[p] * dt;
+        s.dvy += -1.0 * ss * PLN(c.f.e_vel, 1)[p] * dt;
         double ax = c.f.e_alpha[p], ay = PLN(c.f.e_alpha, 1)[p];
         const double g0 = PLN(c.f.e_grad_vel, 0)[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
                      g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
         const double adx = c.rp.alpha_damp_x, ady = c.rp.alpha_damp_y;
         ax += (sy * g0 + sy * g4 - ady * ax) * dt + (sx * g3 + sx * g4 - adx * ax) * dt;
         const double lp = c.f.e_pre[p] + c.f.e_q[p] - PLN(c.f.e_dampref, 2)[p];
-        const double t0 = c.f.e_ste[p], t1 = PLN(c.f.e_ste, 1)[p], t2 = PLN(c.f.e_ste, 2)[p], t3 = PLN(c.f.e_ste, 3)[p];
+        const double t0 = s.st[0], t1 = s.st[1], t2 = s.st[2], t3 = s.st[3];
         const double sd = (t0 - lp) * sy * g0 + t1 * (sy * g1 + sx * g2) + (t2 - lp) * sx * g3 + (sy + sx) * t3 * g4;
         ay += -1.0 * sd * dt - 1.0 * (adx + ady) * ay * dt;
         c.f.e_alpha[p] = ax;
         PLN(c.f.e_alpha, 1)[p] = ay;
+        const int mf = first_material(s, nmat, false);
         #pragma unroll
         for (int m = 1; m < nmat; ++m) {
-            if (PLN(c.f.m_vof, m)[p] < 1.0 - SALEC_TOLVOF) continue;
-            double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
+            if (m != mf) continue;
             if (ty == 1) {
-                const double pt = por ? PLN(c.f.m_pty, m)[p] : 1.0;
-                const double rd = (-(sx + sy) * (*rm - d0) - d0 * ax) * dt;
-                const double ed = (-(sx + sy) * (*em - d1) - ay) * dt;
-                *rm += rd / pt;
-                *em += ed / pt;
+                const double pt = por ? s.pty[m] : 1.0;
+                const double rd = (-(sx + sy) * (s.rho[m] - d0) - d0 * ax) * dt;
+                const double ed = (-(sx + sy) * (s.eng[m] - d1) - ay) * dt;
+                s.rho[m] += rd / pt;
+                s.eng[m] += ed / pt;
             } else {
-                const double rd = (-(sx + sy) * (*rm - d0)) * dt;
-                const double ed = (-(sx + sy) * (*em - d1) - ay) * dt;
-                *rm += rd;
-                *em += ed;
+                const double rd = (-(sx + sy) * (s.rho[m] - d0)) * dt;
+                const double ed = (-(sx + sy) * (s.eng[m] - d1) - ay) * dt;
+                s.rho[m] += rd;
+                s.eng[m] += ed;
             }
-            break;
         }
+        return true;
     } else if (ty == 3) {
         // damp_on_cell_sbc (src/velocity.c:658-767); "+=" in y and "=" in x as in the reference
+        bool changed = false;
         if (sy < 1.0) {
             #pragma unroll
             for (int m = 1; m < nmat; ++m) {
-                if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
-                double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
-                const double dd = *rm - d0, de = *em - d1;
-                *rm += dd * sy + d0;
-                *em += de * sy + d1;
+                if (s.vof[m] < SALEC_TOLVOF) continue;
+                const double dd = s.rho[m] - d0, de = s.eng[m] - d1;
+                s.rho[m] += dd * sy + d0;
+                s.eng[m] += de * sy + d1;
+                changed = true;
             }
         }
         if (sx < 1.0) {
             #pragma unroll
             for (int m = 1; m < nmat; ++m) {
-                if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
-                double *rm = PLN(c.f.m_den, m) + p, *em = PLN(c.f.m_eng, m) + p;
-                const double dd = *rm - d0, de = *em - d1;
-                *rm = dd * sx + d0;
-                *em = de * sx * sx + d1;
+                if (s.vof[m] < SALEC_TOLVOF) continue;
+                const double dd = s.rho[m] - d0, de = s.eng[m] - d1;
+                s.rho[m] = dd * sx + d0;
+                s.eng[m] = de * sx * sx + d1;
+                changed = true;
             }
         }
+        return changed;
     }
+    return false;
 }
 
-__device__ void ejecta_drag_cell(const Ctx &c, int i, int j, long long p, double dt)
+// ejecta_flow (src/ejecta.c:65-133); launched only when resistance or friction is positive
+template <int NM, bool POR>
+__device__ __forceinline__ void ejecta_drag_cell(const Ctx &c, int i, int j, long long p, double dt,
+                                                 CellState<NM, POR> &s)
 {
-    // ejecta_flow (src/ejecta.c:65-133); inactive unless resistance or friction is positive
     const double ey = PLN(c.f.e_pos, 1)[p];
     const double gy = 0.5 * PLN(c.f.v_bf, 1)[KIDX(i - 1, j - 1)] + 0.5 * PLN(c.f.v_bf, 1)[KIDX(i, j - 1)];
     double gyy = 0.;
     gyy += gy;
-    if (ey <= c.f.y_profile[i] && c.f.e_ejt[p] > 0.1) {
+    if (ey <= c.f.y_profile[i] && s.ejt > 0.1) {
         if (c.rp.flow_resistance > 0.) {
-            c.f.e_dvel[p] += -c.rp.flow_resistance * dt * c.f.e_vel[p];
-            PLN(c.f.e_dvel, 1)[p] += -c.rp.flow_resistance * dt * PLN(c.f.e_vel, 1)[p];
+            s.dvx += -c.rp.flow_resistance * dt * c.f.e_vel[p];
+            s.dvy += -c.rp.flow_resistance * dt * PLN(c.f.e_vel, 1)[p];
         }
         if (c.rp.flow_friction > 0.) {
             #pragma unroll
-            for (int q = 0; q < 4; ++q) PLN(c.f.e_ste, q)[p] = 0.;
-            if (c.f.e_vel[p] >= 0.) c.f.e_dvel[p] += -1.0 * c.rp.flow_friction * fabs(gyy) * dt;
-            else c.f.e_dvel[p] += 1.0 * c.rp.flow_friction * fabs(gyy) * dt;
+            for (int q = 0; q < 4; ++q) s.st[q] = 0.;
+            if (c.f.e_vel[p] >= 0.) s.dvx += -1.0 * c.rp.flow_friction * fabs(gyy) * dt;
+            else s.dvx += 1.0 * c.rp.flow_friction * fabs(gyy) * dt;
         }
     }
 }
 
+// update_state (src/sale2d.c:1635-1742) from the register state
 template <int NM, bool POR>
-__device__ __forceinline__ void state_cell(const Ctx &c, long long p)
+__device__ __forceinline__ void state_cell(const Ctx &c, long long p, const CellState<NM, POR> &s)
 {
-    constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
+    constexpr int MM = CellState<NM, POR>::MM;
     const int nmat = NM > 0 ? NM : c.d.nmat;
     constexpr bool por = POR;
-    const double dam = c.f.e_dam[p];
+    const double dam = s.dam;
     double mpre[MM], mcsd[MM], mtem[MM];
     double epre = 0.0, ecsd = 0.0, etem = 0.0, eden = 0.0, emu = 0.0;
     #pragma unroll
     for (int m = 1; m < nmat; ++m) {
-        const double vm = PLN(c.f.m_vof, m)[p];
+        const double vm = s.vof[m];
         if (vm < SALEC_TOLVOF) {
             mpre[m] = 0.; mcsd[m] = 1.; mtem[m] = 0.;
         } else {
-            const DevMat &s = c.mat[m];
-            const double plim = (1.0 - dam) * s.minPint + dam * s.minPdam;
-            const double pt = por ? PLN(c.f.m_pty, m)[p] : 1.0;
-            material_state(s, PLN(c.f.m_den, m)[p], PLN(c.f.m_eng, m)[p], plim, pt, mtem[m], mpre[m], mcsd[m]);
+            const DevMat &ms = c.mat[m];
+            const double plim = (1.0 - dam) * ms.minPint + dam * ms.minPdam;
+            const double pt = por ? s.pty[m] : 1.0;
+            material_state(ms, s.rho[m], s.eng[m], plim, pt, mtem[m], mpre[m], mcsd[m]);
         }
     }
     #pragma unroll
     for (int m = 1; m < nmat; ++m) {
-        const double vm = PLN(c.f.m_vof, m)[p];
-        const double rm = PLN(c.f.m_den, m)[p];
+        const double vm = s.vof[m];
+        const double rm = s.rho[m];
         epre += vm * mpre[m];
         ecsd += vm / dmax(1.0, mcsd[m]);
         etem += vm * mtem[m];
@@ -1341,7 +1455,7 @@ __device__ __forceinline__ void state_cell(const Ctx &c, long long p)
     }
     if (emu > 0.) emu = 1.0 / emu;
     if (ecsd > 0.) ecsd = 1.0 / ecsd;
-    const double v0 = c.f.m_vof[p];
+    const double v0 = s.vof[0];
     if ((c.rp.partpres == 0 && v0 > SALEC_TOLVOF) || (c.rp.partpres == 1 && v0 > 1.0 - SALEC_TOLVOF)) {
         epre = 0.;
         ecsd = 1.0;
@@ -1358,6 +1472,8 @@ __device__ __forceinline__ void state_cell(const Ctx &c, long long p)
     c.f.e_mu[p] = emu;
 }
 
+// One thread per cell: remap (interior), damping (every cell, while t < damp_time), ejecta
+// drag and EOS (interior). The cell's state is stored once, after damping and drag.
 template <int NM, bool POR>
 __global__ void __launch_bounds__(256) k_remap_damp_state(const Ctx c, int do_remap, int do_damp, int do_ejecta, int do_state)
 {
@@ -1366,10 +1482,22 @@ __global__ void __launch_bounds__(256) k_remap_damp_state(const Ctx c, int do_re
     const long long p = KIDX(i, j);
     const bool interior = cell_interior(c, i, j);
     const double dt = c.scal->dt;
-    if (do_remap && interior) remap_cell<NM, POR>(c, i, j, p);
-    if (do_damp && c.rp.damp_time > c.scal->time) damp_cell<NM, POR>(c, p, dt);
-    if (do_ejecta && interior) ejecta_drag_cell(c, i, j, p, dt);
-    if (do_state && interior) state_cell<NM, POR>(c, p);
+    const bool remap = do_remap && interior;
+    const bool damp = do_damp && c.rp.damp_time > c.scal->time && c.rp.damp_type != 4 && c.rp.damp_type != 5;
+    const bool ejecta = do_ejecta && interior;
+    const bool state = do_state && interior;
+    if (!(remap || damp || ejecta || state)) return;
+    CellState<NM, POR> s;
+    if (remap) remap_cell<NM, POR>(c, i, j, p, s);
+    else load_cell<NM, POR>(c, p, s);
+    bool dirty = remap;
+    if (damp) dirty |= damp_cell<NM, POR>(c, p, dt, s);
+    if (ejecta) {
+        ejecta_drag_cell<NM, POR>(c, i, j, p, dt, s);
+        dirty = true;
+    }
+    if (dirty) store_cell<NM, POR>(c, p, s, !state);   // the EOS pass writes e_den itself
+    if (state) state_cell<NM, POR>(c, p, s);
 }
 
 // Launchers: the material count and the porosity switch are template parameters, so that the
@@ -1396,6 +1524,16 @@ void launch_remap_damp_state(const Ctx &c, int do_remap, int do_damp, int do_eje
                              cudaStream_t s)
 {
     SALEC_NM_DISPATCH(k_remap_damp_state, c, do_remap, do_damp, do_ejecta, do_state);
+}
+
+void launch_energy(const Ctx &c, dim3 g, dim3 b, cudaStream_t s)
+{
+    SALEC_NM_DISPATCH(k_energy, c);
+}
+
+void launch_stress(const Ctx &c, dim3 g, dim3 b, cudaStream_t s)
+{
+    SALEC_NM_DISPATCH(k_stress, c);
 }
 
 // ============================================================ phase 15: cycle control

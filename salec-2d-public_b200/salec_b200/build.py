@@ -3,7 +3,7 @@
 The library has no dependency on torch or Python: it is the C ABI of include/salec_gpu.h.
 Flags: ``-gencode arch=compute_100a,code=sm_100a`` (B200 only), ``--fmad=false`` so that no
 multiply-add is contracted (the FP64 form keeps the reference's rounding), ``-lineinfo`` for
-profiling.
+profiling. Links the system zlib for the output files.
 """
 from __future__ import annotations
 
@@ -15,7 +15,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)               # salec-2d-public_b200/
 CSRC = os.path.join(ROOT, "csrc")
 LIB = os.path.join(PKG, "libsalec_b200.so")
-SOURCES = ["salec_step.cu", "salec_runtime.cu", "salec_init.cu", "salec_noalloc.cu", "salec_ghost.cpp"]
+SOURCES = ["salec_step.cu", "salec_runtime.cu", "salec_init.cu", "salec_noalloc.cu", "salec_output.cu",
+           "salec_ghost.cpp"]
 HEADERS = ["salec_device.cuh", "salec_kernels.h", "salec_deck.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "--fmad=false", "-lineinfo",
               "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-warn-spills"]
@@ -40,7 +41,8 @@ def _stale() -> bool:
 def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     if not force and not _stale():
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + (extra or []) + [os.path.join(CSRC, f) for f in SOURCES] + ["-o", LIB + ".tmp"]
+    cmd = ([nvcc()] + NVCC_FLAGS + (extra or []) + [os.path.join(CSRC, f) for f in SOURCES] +
+           ["-lz", "-o", LIB + ".tmp"])
     if verbose:
         print(" ".join(cmd))
     res = subprocess.run(cmd, capture_output=True, text=True)

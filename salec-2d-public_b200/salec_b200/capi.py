@@ -18,6 +18,8 @@ c_d, c_i, c_ll = ctypes.c_double, ctypes.c_int, ctypes.c_longlong
 P_D = ctypes.POINTER(c_d)
 
 SALEC_OK = 0
+OUT_WAIT = 1          # salec_gpu_write_output flags
+OUT_TRACER_TXT = 2
 STATUS = {0: "SALEC_OK", -1: "SALEC_ERR_ARG", -2: "SALEC_ERR_CUDA", -3: "SALEC_ERR_ALLOC",
           -4: "SALEC_ERR_STATE", -5: "SALEC_ERR_UNSUPPORTED", -6: "SALEC_ERR_NUMERIC"}
 EOS_ANEOS, EOS_TILLOTSON, EOS_SIEDEN = 0, 1, 2
@@ -85,6 +87,8 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_set_tracers": ([vp, c_i, P_D], c_i),
             "salec_gpu_get_tracers": ([vp, P_D, ctypes.POINTER(c_i)], c_i),
             "salec_gpu_check": ([vp, ctypes.POINTER(c_ll)], c_i),
+            "salec_gpu_write_output": ([vp, ctypes.c_char_p, ctypes.c_char_p, c_i, c_i, c_i], c_i),
+            "salec_gpu_output_wait": ([vp], c_i),
             "salec_gpu_func_index": ([ctypes.c_char_p], c_i),
             "salec_gpu_create_from_deck": ([ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(vp)], c_i),
             "salec_gpu_get_run": ([vp, ctypes.POINTER(RunDesc)], c_i),
@@ -275,6 +279,18 @@ class Simulation:
 
     def set_scalar(self, name: str, value: float) -> None:
         _check(lib().salec_gpu_set_scalar(self.h, name.encode(), float(value)), "set_scalar " + name)
+
+    def write_output(self, folder: str, prefix: str, out_step: int, rank: int = 0, wait: bool = True,
+                     tracer_txt: bool = False) -> None:
+        """Write the reference's .vts/.vtp (and optional tracer .txt) files of the current state
+        under folder/vts, folder/vtp, folder/txt. Without wait the files are written by host
+        threads while the device continues; output_wait() joins them."""
+        flags = (OUT_WAIT if wait else 0) | (OUT_TRACER_TXT if tracer_txt else 0)
+        _check(lib().salec_gpu_write_output(self.h, folder.encode(), prefix.encode(), rank, out_step, flags),
+               "salec_gpu_write_output")
+
+    def output_wait(self) -> None:
+        _check(lib().salec_gpu_output_wait(self.h), "salec_gpu_output_wait")
 
     def check(self) -> int:
         n = c_ll()

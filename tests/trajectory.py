@@ -75,3 +75,40 @@ def simulation_from_record(rec: Dict):
 def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     nb = float(np.linalg.norm(b))
     return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
+
+
+def oracle_output_case(kind: str, nsteps: int, folder: str) -> Dict:
+    """The reference's own output files of a mid-cycle state: nsteps cycles, then phases 0-13
+    (the point where src/salec2d.c writes its VTK files), then sale2d_write_vtk/_vtp. Returns
+    the state at that point (to load into the GPU library) and the bytes of every written file."""
+    deck, folder = bridge.write_small_deck(kind, folder)
+    run_dir = os.path.join(folder, "run")
+    ref.init(deck, folder, run_dir)
+    ref.step(nsteps)
+    ref.phases(0, 13)
+    run = bridge.run_desc_from_oracle()
+    out = {
+        "run": {n: (list(getattr(run, n)) if n == "go" else getattr(run, n)) for n in RUN_FIELDS},
+        "mats": bridge.materials_from_oracle(run.nmat),
+        "init": {n: ref.get(n) for n in bridge.UPLOAD_FIELDS},
+        "tracers0": ref.tracers(),
+        "files": {},
+    }
+    for sub in ("vts", "vtp", "txt"):
+        d = os.path.join(run_dir, sub)
+        for f in os.listdir(d):
+            os.unlink(os.path.join(d, f))
+    ref.write_output()
+    for sub in ("vts", "vtp", "txt"):
+        d = os.path.join(run_dir, sub)
+        for f in sorted(os.listdir(d)):
+            with open(os.path.join(d, f), "rb") as fh:
+                out["files"][sub + "/" + f] = fh.read()
+    return out
+
+
+def oracle_output_cases(kinds: List[str], nsteps: int, root: str) -> Dict[str, Dict]:
+    ctx = mp.get_context("spawn")
+    with cf.ProcessPoolExecutor(max_workers=max(1, min(len(kinds), os.cpu_count() or 1)), mp_context=ctx) as ex:
+        futs = {k: ex.submit(oracle_output_case, k, nsteps, os.path.join(root, k)) for k in kinds}
+        return {k: f.result() for k, f in futs.items()}
