@@ -185,6 +185,17 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
+
+
+def crater_depth(profile: np.ndarray, surface: float, ncols: int = 4) -> float:
+    """Transient crater depth from the surface profile: the lowest surface height over the
+    columns next to the symmetry axis, below the pre-impact surface."""
+    return float(surface - np.min(profile[2:2 + ncols]))
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -371,6 +382,56 @@ def run_gpu_arm(args):
     e2e = world * cells * args.steps / e2e_s
     nbad = sim.check()
 
+    # mixed form (FP32 storage of the relaxed fields): same deck, same warm-up and timed steps,
+    # then its state against the plain FP64 form after the same number of cycles from the start
+    mixed = None
+    if not args.no_mixed:
+        mix = capi.Simulation.from_deck(deck, tmp, precision=capi.PRECISION_MIXED)
+        mix.step(args.warmup)
+        mix.sync()
+        mstream = torch.cuda.ExternalStream(mix.stream())
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(mstream)
+        mix.step(args.steps)
+        e1.record(mstream)
+        e1.synchronize()
+        mms = all_max(e0.elapsed_time(e1))
+        mvalue = world * cells * args.steps / (mms / 1000.0)
+        for name, a in init_state.items():
+            sim.set_field(name, a)
+        sim.set_tracers(init_tracers)
+        sim.set_scalar("dt", run.dt)
+        sim.set_scalar("time", 0.0)
+        sim.step(args.warmup + args.steps)
+        fields_cmp = ("e_den", "e_pre", "m_eng", "m_vof", "v_vel")
+        ref_state = {n: sim.get_field(n) for n in fields_cmp}
+        ref_profile = sim.get_field("y_profile").reshape(-1)
+        errs = {n: rel_l2(mix.get_field(n), ref_state[n]) for n in fields_cmp}
+        # sensitivity of the FP64 form itself: the same run with m_den and m_eng perturbed by 1e-7
+        # relative at the start (the size of one FP32 rounding)
+        for name, a in init_state.items():
+            sim.set_field(name, a * (1.0 + 1e-7) if name in ("m_den", "m_eng") else a)
+        sim.set_tracers(init_tracers)
+        sim.set_scalar("dt", run.dt)
+        sim.set_scalar("time", 0.0)
+        sim.step(args.warmup + args.steps)
+        sens = {n: rel_l2(sim.get_field(n), ref_state[n]) for n in fields_cmp}
+        prof64 = ref_profile
+        surface = float(np.median(prof64[2:-2]))   # most columns are still at the pre-impact surface
+        d64 = crater_depth(prof64, surface)
+        d32 = crater_depth(mix.get_field("y_profile").reshape(-1), surface)
+        mixed = {"value": mvalue, "unit": "cell-updates/s", "ms_per_step": mms / args.steps,
+                 "speedup_vs_fp64": mvalue / value,
+                 "storage": "FP32 relaxed fields, FP64 m_vof/m_den/m_eng/m_pty/e_cvs/positions/volumes/face records",
+                 "arithmetic": "f64",
+                 "rel_l2_vs_fp64": errs, "cycles_compared": args.warmup + args.steps,
+                 "fp64_sensitivity_rel_l2": sens,
+                 "crater_depth_m": {"fp64": max(d64, 0.0), "mixed": max(d32, 0.0),
+                                    "rel_err": abs(d32 - d64) / d64 if d64 > 0 else None},
+                 "nonfinite": mix.check()}
+        mix.close()
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         with tempfile.TemporaryDirectory() as ctmp:
@@ -406,6 +467,7 @@ def run_gpu_arm(args):
             "clocks": clocks,
             "cpu_baseline": cpu,
             "nonfinite": nbad,
+            "mixed": mixed,
         }
         print(json.dumps(line), flush=True)
     sim.close()
@@ -424,6 +486,7 @@ def main():
     ap.add_argument("--cpu-n", type=int, default=256, help="cells per side of the CPU sample")
     ap.add_argument("--cpu-steps", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
     args = ap.parse_args()
     if args.warmup < 1:
         args.warmup = 1

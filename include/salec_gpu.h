@@ -76,7 +76,17 @@ typedef struct salec_run_desc {
     double tracer_lub_y0, tracer_lub_frac;
     double max_dt, dt, time;    /* cycle.maxdt, current dt and simulated time */
     int i_step;
+    /* Storage precision of the device mesh (no counterpart in the reference, which is FP64):
+     * SALEC_PRECISION_FP64 (0, the plain form, bit-parity with the reference) or
+     * SALEC_PRECISION_MIXED (1): the fields of stress, strain rate, viscosity, EOS outputs,
+     * velocities, accelerations, damping and geometry weights are stored as FP32 and computed in
+     * FP64 registers; volume fractions, material densities and energies, the porosity state,
+     * positions, cell volumes and the face flux records (volume-fraction advection, mass and
+     * energy conservation) stay FP64. Zero-initialised descriptions select FP64. */
+    int precision;
 } salec_run_desc;
+
+enum salec_precision { SALEC_PRECISION_FP64 = 0, SALEC_PRECISION_MIXED = 1 };
 
 /*
  * One material (index >= 1; index 0 is vacuum and is ignored): the reference's
@@ -120,6 +130,8 @@ int salec_gpu_destroy(salec_gpu *h);
  * domain of (npgx*npx) x (npgy*npy) cells.
  */
 int salec_gpu_create_from_deck(const char *deck_path, const char *eos_dir, salec_gpu **out);
+/* The same with a storage precision (salec_precision) for the device mesh. */
+int salec_gpu_create_from_deck_ex(const char *deck_path, const char *eos_dir, int precision, salec_gpu **out);
 /* The run description of a handle (for a deck-created handle: the values derived from the deck). */
 int salec_gpu_get_run(const salec_gpu *h, salec_run_desc *out);
 

@@ -76,18 +76,34 @@ struct Scal {
     unsigned long long aux;       // ordered-bits MAX accumulator used at initialisation
 };
 
-struct Fields {
+// Device planes of every field. R is the storage type of the "relaxed" fields: double in the
+// plain FP64 form, float in the mixed form. The fields that carry volume-fraction advection,
+// mass and energy conservation and the mesh positions stay FP64 in both forms (m_vof, m_den,
+// m_eng, v_pos, e_pos, e_vol, the face records bx_phi/by_phi and the surface profile), and so
+// do the porosity state (distension m_pty and cold volume strain e_cvs): the compaction law is
+// evaluated next to its thresholds (alpha0, epse0), where FP32 rounding of the distension
+// moves it across them.
+// Every member is a pointer, so all instances share one layout.
+template <class R>
+struct FieldsT {
     // vertices
-    double *v_vel, *v_bf, *v_acc, *v_dis, *v_pos, *v_vof, *v_mass, *v_vol, *v_subvol, *v_laplace,
-        *v_suf, *v_alpha, *v_beta;
+    R *v_vel, *v_bf, *v_acc, *v_dis;
+    double *v_pos;
+    R *v_vof, *v_mass, *v_vol, *v_subvol, *v_laplace, *v_suf, *v_alpha, *v_beta;
     // cells
-    double *e_vel, *e_div_vel, *e_grad_vel, *e_ste, *e_mu, *e_dvel, *e_pre, *e_tem, *e_den,
-        *e_eng, *e_csd, *e_dam, *e_cvs, *m_vof, *m_den, *m_eng, *m_pty, *e_wpt, *e_pos, *e_vol,
-        *e_suf, *e_grad, *e_subvol, *e_q, *e_strength, *e_cnd, *e_tps, *e_ste2s, *e_sta2s,
-        *e_alpha, *e_beta, *e_sigma, *e_dampref, *e_vib, *e_ejt;
+    R *e_vel, *e_div_vel, *e_grad_vel, *e_ste, *e_mu, *e_dvel, *e_pre, *e_tem, *e_den, *e_eng, *e_csd, *e_dam;
+    double *e_cvs, *m_vof, *m_den, *m_eng, *m_pty;
+    R *e_wpt;
+    double *e_pos, *e_vol;
+    R *e_suf, *e_grad, *e_subvol, *e_q, *e_strength, *e_cnd, *e_tps, *e_ste2s, *e_sta2s, *e_alpha, *e_beta,
+        *e_sigma, *e_dampref, *e_vib, *e_ejt;
     // faces and columns
-    double *bx_phi, *by_phi, *bx_normal, *by_normal, *y_profile;
+    double *bx_phi, *by_phi;
+    R *bx_normal, *by_normal;
+    double *y_profile;
 };
+using Fields = FieldsT<double>;
+static_assert(sizeof(FieldsT<float>) == sizeof(FieldsT<double>), "field tables share one layout");
 
 // Lagrangian tracers as structure-of-arrays in the reference's list order
 // (tracer_t of src/mpi_vec/linked_list.h:17-27 plus the cell index and a live flag).
@@ -98,14 +114,17 @@ struct Tracers {
     int n;
 };
 
-struct Ctx {
+template <class R>
+struct CtxT {
+    using real = R;
     Dims d;
-    Fields f;
+    FieldsT<R> f;
     RunParams rp;
     const DevMat *mat;
     Scal *scal;
     Tracers tr;
 };
+using Ctx = CtxT<double>;
 
 // ------------------------------------------------------------------ small helpers
 __host__ __device__ __forceinline__ double dmin(double a, double b) { return a < b ? a : b; }   // MIN / Min

@@ -1502,6 +1502,12 @@ int salec_internal_fail(int code, const char *msg);
 
 extern "C" int salec_gpu_create_from_deck(const char *deck_path, const char *eos_dir, salec_gpu **out)
 {
+    return salec_gpu_create_from_deck_ex(deck_path, eos_dir, SALEC_PRECISION_FP64, out);
+}
+
+extern "C" int salec_gpu_create_from_deck_ex(const char *deck_path, const char *eos_dir, int precision,
+                                             salec_gpu **out)
+{
     using namespace salec;
     if (!deck_path || !eos_dir || !out) return salec_internal_fail(SALEC_ERR_ARG, "null argument");
     *out = nullptr;
@@ -1517,6 +1523,7 @@ extern "C" int salec_gpu_create_from_deck(const char *deck_path, const char *eos
     if (rc) return salec_internal_fail(rc, err.c_str());
 
     salec_run_desc run{};
+    run.precision = precision;
     run.nx = S.npgx * S.nx;
     run.ny = S.npgy * S.ny;
     run.nmat = S.nmat;

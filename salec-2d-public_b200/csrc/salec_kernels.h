@@ -5,16 +5,18 @@
 
 namespace salec {
 
-struct Ctx;
+template <class R>
+struct CtxT;   // salec_device.cuh
 
 #define SALEC_MAX_GATHER_FIELDS 8
 
 // Boundary fills as gathers: for entry k, dst[k] <- op_c(src[k]) for each component c, where
 // op_c is 3 bits of ops[k]: 0 copy, 1 negate, 2 abs, 3 -abs, 4 +0.0, 5 -0.0.
 struct GatherField {
-    double *base;          // component-0 plane of the field
-    long long plane;       // plane stride
+    void *base;            // component-0 plane of the field (double, or float when f32)
+    long long plane;       // plane stride in elements
     int ncomp, ncomp_max;  // components of this field; max over the batch (scratch stride)
+    int f32;               // the field is stored as float
     const int *dst, *src;
     const unsigned *ops;
 };
@@ -41,31 +43,25 @@ GatherMap build_ghost_map(int enx, int eny, int P, int ncomp, const int go[4], G
 // Build the gather map of the vertex restriction table (vnx x vny points, pitch P).
 GatherMap build_restrict_map(int vnx, int vny, int P, int ncomp, const int go[4]);
 
+// Step kernels of salec_step.cu, launched over their own grids by launch_step_kernel; R is
+// the storage type of the relaxed fields (double: plain FP64 form, float: mixed form).
+enum StepKernel {
+    SK_PROFILE_RESET, SK_TRACE_PROFILE, SK_PROFILE_DECODE, SK_VERTEX_VOF_MOMENTUM, SK_CELL_VELOCITY,
+    SK_VOID_VERTICES, SK_GRADIENT, SK_FINALIZE_DT, SK_STRESS, SK_ACCELERATION, SK_DISPLACEMENT, SK_ENERGY,
+    SK_TRACERS, SK_FLUX, SK_REMAP_DAMP_STATE, SK_CYCLE, SK_RECORD_REFERENCE, SK_INIT_VERTEX_VELOCITY
+};
+
 #ifdef __CUDACC__
-// kernels (salec_step.cu)
-__global__ void k_profile_reset(const Ctx c);
-__global__ void k_trace_profile(const Ctx c);
-__global__ void k_profile_decode(const Ctx c);
-__global__ void k_vertex_vof_momentum(const Ctx c);
-__global__ void k_cell_velocity(const Ctx c);
-__global__ void k_void_vertices(const Ctx c);
-__global__ void k_gradient_viscosity_cfl(const Ctx c);
-__global__ void k_finalize_dt(const Ctx c);
-__global__ void k_vertex_acceleration(const Ctx c);
-__global__ void k_vertex_displacement(const Ctx c);
-__global__ void k_tracers(const Ctx c);
-__global__ void k_cycle(const Ctx c);
-__global__ void k_record_reference_state(const Ctx c);
-__global__ void k_init_vertex_velocity(const Ctx c);
+// flux: a0 = pass (0 interior, 1 pad); remap: a0..a3 = remap, damping, ejecta drag, EOS switches
+template <class R>
+void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, int a0 = 0, int a1 = 0, int a2 = 0,
+                        int a3 = 0);
 __global__ void k_gather(GatherBatch g, int mode, double *scratch);
-__global__ void k_aos_to_planes(const double *aos, double *base, long long plane, int P, int nx, int ny, int nc);
-__global__ void k_planes_to_aos(const double *base, double *aos, long long plane, int P, int nx, int ny, int nc);
-__global__ void k_count_nonfinite(const double *base, long long n, unsigned long long *out);
-void launch_stress(const Ctx &c, dim3 g, dim3 b, cudaStream_t s);
-void launch_energy(const Ctx &c, dim3 g, dim3 b, cudaStream_t s);
-void launch_flux(const Ctx &c, int pass, dim3 g, dim3 b, cudaStream_t s);
-void launch_remap_damp_state(const Ctx &c, int do_remap, int do_damp, int do_ejecta, int do_state, dim3 g, dim3 b,
-                             cudaStream_t s);
+void launch_aos_to_planes(const double *aos, void *base, bool f32, long long plane, int P, int nx, int ny, int nc,
+                          cudaStream_t s);
+void launch_planes_to_aos(const void *base, bool f32, double *aos, long long plane, int P, int nx, int ny, int nc,
+                          cudaStream_t s);
+void launch_count_nonfinite(const void *base, bool f32, long long n, unsigned long long *out, cudaStream_t s);
 #endif
 
 } // namespace salec

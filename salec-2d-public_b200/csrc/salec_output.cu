@@ -31,8 +31,8 @@ using namespace salec;
 
 struct salec_gpu;
 int salec_internal_fail(int code, const char *msg);
-int salec_internal_field_view(salec_gpu *h, const char *name, const double **base, long long *plane, int *pitch,
-                              int *nx, int *ny, int *nc);
+int salec_internal_field_view(salec_gpu *h, const char *name, const void **base, int *f32, long long *plane,
+                              int *pitch, int *nx, int *ny, int *nc);
 cudaStream_t salec_internal_stream(salec_gpu *h);
 Tracers salec_internal_tracers(salec_gpu *h);
 Dims salec_internal_dims(salec_gpu *h);
@@ -45,11 +45,12 @@ constexpr int kMaxSeg = 32;
 constexpr int kTracerCols = 14;   // matid tag gx gy vx vy den tem pre mpre mtem x y z
 
 struct PackSeg {
-    const double *base;
+    const void *base;  // double planes, or float planes when f32
     long long plane;   // doubles between components
     long long out;     // first float of this array in the staging buffer
     long long start;   // first point of this segment in the batch
     int pitch, nx, ny, nc, oc;   // oc = output components per point (3 for coordinates)
+    int f32;
 };
 
 struct PackBatch {
@@ -70,13 +71,24 @@ __global__ void k_pack_points(PackBatch b, float *out)
         const int x = (int)(q % g.nx), y = (int)(q / g.nx);
         const long long src = x + (long long)g.pitch * y;
         float *o = out + g.out + q * g.oc;
-        for (int c = 0; c < g.nc; ++c) o[c] = __double2float_rn(g.base[c * g.plane + src]);
+        if (g.f32) {
+            const float *b = static_cast<const float *>(g.base);
+            for (int c = 0; c < g.nc; ++c) o[c] = b[c * g.plane + src];
+        } else {
+            const double *b = static_cast<const double *>(g.base);
+            for (int c = 0; c < g.nc; ++c) o[c] = __double2float_rn(b[c * g.plane + src]);
+        }
         for (int c = g.nc; c < g.oc; ++c) o[c] = 0.0f;
     }
 }
 
 // One row of the tracer export per tracer slot; slots of deleted tracers get live = 0.
-__global__ void k_pack_tracers(Tracers T, const double *e_den, const double *e_tem, const double *e_pre, int pitch,
+__device__ __forceinline__ float value_f32(const void *base, int f32, long long k)
+{
+    return f32 ? static_cast<const float *>(base)[k] : __double2float_rn(static_cast<const double *>(base)[k]);
+}
+
+__global__ void k_pack_tracers(Tracers T, const void *e_den, const void *e_tem, const void *e_pre, int f32, int pitch,
                                float *rows, int *live)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -90,9 +102,9 @@ __global__ void k_pack_tracers(Tracers T, const double *e_den, const double *e_t
     r[3] = 1.0f * T.gy[t];
     r[4] = __double2float_rn(T.vx[t]);
     r[5] = __double2float_rn(T.vy[t]);
-    r[6] = T.alive[t] ? __double2float_rn(e_den[cell]) : 0.0f;
-    r[7] = T.alive[t] ? __double2float_rn(e_tem[cell]) : 0.0f;
-    r[8] = T.alive[t] ? __double2float_rn(e_pre[cell]) : 0.0f;
+    r[6] = T.alive[t] ? value_f32(e_den, f32, cell) : 0.0f;
+    r[7] = T.alive[t] ? value_f32(e_tem, f32, cell) : 0.0f;
+    r[8] = T.alive[t] ? value_f32(e_pre, f32, cell) : 0.0f;
     r[9] = T.mpre[t];
     r[10] = T.mtem[t];
     r[11] = __double2float_rn(T.x[t]);
@@ -410,7 +422,8 @@ extern "C" int salec_gpu_write_output(salec_gpu *h, const char *dir, const char 
     for (const Item &it : items) {
         PackSeg &g = b.seg[b.nseg++];
         int nx, ny, nc;
-        if ((rc = salec_internal_field_view(h, it.field, &g.base, &g.plane, &g.pitch, &nx, &ny, &nc))) return rc;
+        if ((rc = salec_internal_field_view(h, it.field, &g.base, &g.f32, &g.plane, &g.pitch, &nx, &ny, &nc)))
+            return rc;
         g.nx = nx; g.ny = ny; g.nc = nc;
         g.oc = it.section == 2 ? 3 : nc;
         g.out = off;
@@ -443,13 +456,14 @@ extern "C" int salec_gpu_write_output(salec_gpu *h, const char *dir, const char 
     k_pack_points<<<nb, tb, 0, s>>>(b, W->dev);
     int launches = 1;
     if (T.n > 0) {
-        const double *den, *tem, *pre;
+        const void *den, *tem, *pre;
         long long pl;
-        int pitch, nx, ny, nc;
-        salec_internal_field_view(h, "e_den", &den, &pl, &pitch, &nx, &ny, &nc);
-        salec_internal_field_view(h, "e_tem", &tem, &pl, &pitch, &nx, &ny, &nc);
-        salec_internal_field_view(h, "e_pre", &pre, &pl, &pitch, &nx, &ny, &nc);
-        k_pack_tracers<<<(T.n + 127) / 128, 128, 0, s>>>(T, den, tem, pre, pitch, W->dev + J.tracer_off, W->dev_live);
+        int pitch, nx, ny, nc, f32;
+        salec_internal_field_view(h, "e_den", &den, &f32, &pl, &pitch, &nx, &ny, &nc);
+        salec_internal_field_view(h, "e_tem", &tem, &f32, &pl, &pitch, &nx, &ny, &nc);
+        salec_internal_field_view(h, "e_pre", &pre, &f32, &pl, &pitch, &nx, &ny, &nc);
+        k_pack_tracers<<<(T.n + 127) / 128, 128, 0, s>>>(T, den, tem, pre, f32, pitch, W->dev + J.tracer_off,
+                                                          W->dev_live);
         ++launches;
     }
     salec_internal_add_launches(h, launches);

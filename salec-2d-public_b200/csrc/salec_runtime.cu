@@ -72,6 +72,16 @@ const FieldInfo kFields[] = {
 #undef F_
 constexpr int kNumFields = sizeof(kFields) / sizeof(kFields[0]);
 
+// Fields kept FP64 in the mixed form (FieldsT in salec_device.cuh).
+bool field_exact(int k)
+{
+    static const char *exact[] = {"v_pos", "m_vof", "m_den", "m_eng", "m_pty", "e_cvs", "e_pos", "e_vol",
+                                  "bx_phi", "by_phi", "y_profile"};
+    for (const char *e : exact)
+        if (strcmp(kFields[k].name, e) == 0) return true;
+    return false;
+}
+
 int field_by_name(const char *n)
 {
     if (!n) return -1;
@@ -101,8 +111,9 @@ struct salec_gpu {
     RunParams rp{};
     int go[4] = {0, 0, 0, 0};
     cudaStream_t stream = nullptr;
-    double *pool = nullptr;
-    size_t pool_doubles = 0;
+    char *pool = nullptr;
+    size_t pool_bytes = 0;
+    int mixed = 0;              // 1: relaxed fields stored as float (mixed form)
     Fields f{};
     DevMat *mat = nullptr;
     std::vector<void *> owned;   // device allocations besides the pool
@@ -124,17 +135,19 @@ struct salec_gpu {
     long long launches = 0;     // kernels launched by this handle
     void *output = nullptr;     // output writer state (salec_output.cu)
 
-    Ctx ctx() const
+    template <class R>
+    CtxT<R> ctx_t() const
     {
-        Ctx c;
+        CtxT<R> c;
         c.d = d;
-        c.f = f;
+        memcpy(&c.f, &f, sizeof(c.f));   // same pointers; relaxed ones address floats in the mixed form
         c.rp = rp;
         c.mat = mat;
         c.scal = scal;
         c.tr = tr;
         return c;
     }
+    Ctx ctx() const { return ctx_t<double>(); }
 };
 
 namespace {
@@ -157,6 +170,9 @@ void field_points(const salec_gpu *h, int k, int &nx, int &ny)
     default: nx = h->d.enx; ny = 1; break;
     }
 }
+
+bool field_f32(const salec_gpu *h, int k) { return h->mixed && !field_exact(k); }
+size_t field_elem(const salec_gpu *h, int k) { return field_f32(h, k) ? sizeof(float) : sizeof(double); }
 
 double *&field_ptr(salec_gpu *h, int k)
 {
@@ -186,6 +202,7 @@ int make_gather(salec_gpu *h, Gather &g, const std::vector<std::pair<int, Gather
         const GatherMap &m = maps[k].second;
         GatherField &gf = g.batch.field[k];
         gf.base = field_ptr(h, fid);
+        gf.f32 = field_f32(h, fid) ? 1 : 0;
         gf.plane = h->d.PL;
         gf.ncomp = field_ncomp(h, fid);
         gf.ncomp_max = g.ncomp_max;
@@ -220,71 +237,66 @@ int run_gather(salec_gpu *h, const Gather &g)
     return SALEC_OK;
 }
 
-dim3 grid2(int nx, int ny, dim3 b) { return dim3((nx + b.x - 1) / b.x, (ny + b.y - 1) / b.y); }
-
-int run_phase(salec_gpu *h, int ph)
+template <class R>
+int run_phase_t(salec_gpu *h, int ph)
 {
-    const Ctx c = h->ctx();
-    const dim3 blk(32, 8);
-    const dim3 gc = grid2(h->d.enx, h->d.eny, blk), gv = grid2(h->d.vnx, h->d.vny, blk);
+    const CtxT<R> c = h->ctx_t<R>();
     cudaStream_t s = h->stream;
     int rc = SALEC_OK;
     static const int kLaunches[16] = {3, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1, 0, 2, 0, 1, 1};
     h->launches += kLaunches[ph] + (ph == 11 && h->tr.n > 0 ? 1 : 0);
     switch (ph) {
-    case 0: {
-        const int nb = (h->d.enx + 255) / 256;
-        k_profile_reset<<<nb, 256, 0, s>>>(c);
-        k_trace_profile<<<dim3((h->d.enx + 31) / 32, (h->d.eny + 63) / 64), blk, 0, s>>>(c);
-        k_profile_decode<<<nb, 256, 0, s>>>(c);
+    case 0:
+        launch_step_kernel(SK_PROFILE_RESET, c, s);
+        launch_step_kernel(SK_TRACE_PROFILE, c, s);
+        launch_step_kernel(SK_PROFILE_DECODE, c, s);
         break;
-    }
     case 1:   // vertex volume fractions and vertex momentum in one sweep (phase 2 is empty)
         rc = run_gather(h, h->g_mvof);
         if (!rc) rc = run_gather(h, h->g_dvel_den);
-        k_vertex_vof_momentum<<<gv, blk, 0, s>>>(c);
+        launch_step_kernel(SK_VERTEX_VOF_MOMENTUM, c, s);
         if (!rc) rc = run_gather(h, h->r_vel);
         break;
     case 2: break;
     case 3:
-        k_cell_velocity<<<gc, blk, 0, s>>>(c);
+        launch_step_kernel(SK_CELL_VELOCITY, c, s);
         rc = run_gather(h, h->g_evel);
         break;
-    case 4: k_void_vertices<<<gv, blk, 0, s>>>(c); break;
-    case 5: k_gradient_viscosity_cfl<<<gc, blk, 0, s>>>(c); break;
-    case 6: k_finalize_dt<<<1, 32, 0, s>>>(c); break;
-    case 7: launch_stress(c, gc, blk, s); break;
+    case 4: launch_step_kernel(SK_VOID_VERTICES, c, s); break;
+    case 5: launch_step_kernel(SK_GRADIENT, c, s); break;
+    case 6: launch_step_kernel(SK_FINALIZE_DT, c, s); break;
+    case 7: launch_step_kernel(SK_STRESS, c, s); break;
     case 8:
         rc = run_gather(h, h->g_pre_ste_q);
-        k_vertex_acceleration<<<gv, blk, 0, s>>>(c);
+        launch_step_kernel(SK_ACCELERATION, c, s);
         if (!rc) rc = run_gather(h, h->r_acc);
         break;
     case 9:
-        k_vertex_displacement<<<gv, blk, 0, s>>>(c);
+        launch_step_kernel(SK_DISPLACEMENT, c, s);
         rc = run_gather(h, h->r_dis);
         break;
-    case 10: launch_energy(c, gc, blk, s); break;
-    case 11:
-        if (h->tr.n > 0) k_tracers<<<(h->tr.n + 127) / 128, 128, 0, s>>>(c);
-        break;
+    case 10: launch_step_kernel(SK_ENERGY, c, s); break;
+    case 11: launch_step_kernel(SK_TRACERS, c, s); break;
     case 12:
-        launch_flux(c, 0, gc, blk, s);
+        launch_step_kernel(SK_FLUX, c, s, 0);
         rc = run_gather(h, h->g_flux_state);
-        launch_flux(c, 1, gc, blk, s);
+        launch_step_kernel(SK_FLUX, c, s, 1);
         break;
     case 13: break;   // strength condition from tracers (lubrication is rejected at create)
     case 14: {
         const int ejecta = (h->rp.flow_resistance > 0. || h->rp.flow_friction > 0.) ? 1 : 0;
-        launch_remap_damp_state(c, 1, 1, ejecta, 1, gc, blk, s);
+        launch_step_kernel(SK_REMAP_DAMP_STATE, c, s, 1, 1, ejecta, 1);
         break;
     }
-    case 15: k_cycle<<<1, 32, 0, s>>>(c); break;
+    case 15: launch_step_kernel(SK_CYCLE, c, s); break;
     default: return fail(SALEC_ERR_ARG, "phase out of range");
     }
     if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
     return SALEC_OK;
 }
+
+int run_phase(salec_gpu *h, int ph) { return h->mixed ? run_phase_t<float>(h, ph) : run_phase_t<double>(h, ph); }
 
 int build_gathers(salec_gpu *h)
 {
@@ -379,17 +391,16 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
         CUDA_TRY(cudaMalloc(&h->staging, need * sizeof(double)));
         h->staging_doubles = need;
     }
-    double *base = field_ptr(h, fid);
+    void *base = field_ptr(h, fid);
+    const bool f32 = field_f32(h, fid);
     const long long plane = kFields[fid].loc == L_COL ? 0 : h->d.PL;
-    const int tb = 256;
-    const int nb = (int)(((long long)nx * ny + tb - 1) / tb);
     if (to_device) {
         CUDA_TRY(cudaMemcpyAsync(h->staging, host, need * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        k_aos_to_planes<<<nb, tb, 0, h->stream>>>(h->staging, base, plane, h->d.P, nx, ny, nc);
+        launch_aos_to_planes(h->staging, base, f32, plane, h->d.P, nx, ny, nc, h->stream);
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaStreamSynchronize(h->stream));
     } else {
-        k_planes_to_aos<<<nb, tb, 0, h->stream>>>(base, h->staging, plane, h->d.P, nx, ny, nc);
+        launch_planes_to_aos(base, f32, h->staging, plane, h->d.P, nx, ny, nc, h->stream);
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaMemcpyAsync(host, h->staging, need * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -414,20 +425,15 @@ void release(salec_gpu *h)
     delete h;
 }
 
-} // namespace
-
-// Last start-up steps on the device (src/salec2d.c:76-94): first EOS call, ghost fills,
-// damping reference state and arrival time, vertex velocities, cleared cell velocities.
-int salec_internal_finish_init(salec_gpu *h, double damp_time_in, double *damp_time_out)
+template <class R>
+int finish_init_t(salec_gpu *h, double damp_time_in, double *damp_time_out)
 {
-    const Ctx c = h->ctx();
-    const dim3 blk(32, 8);
-    const dim3 gc = grid2(h->d.enx, h->d.eny, blk), gv = grid2(h->d.vnx, h->d.vny, blk);
-    launch_remap_damp_state(c, 0, 0, 0, 1, gc, blk, h->stream);
+    const CtxT<R> c = h->ctx_t<R>();
+    launch_step_kernel(SK_REMAP_DAMP_STATE, c, h->stream, 0, 0, 0, 1);
     int rc = run_gather(h, h->g_init);
     if (rc) return rc;
     CUDA_TRY(cudaMemsetAsync(&h->scal->aux, 0, sizeof(unsigned long long), h->stream));
-    k_record_reference_state<<<gc, blk, 0, h->stream>>>(c);
+    launch_step_kernel(SK_RECORD_REFERENCE, c, h->stream);
     CUDA_TRY(cudaGetLastError());
     unsigned long long mx = 0;
     CUDA_TRY(cudaMemcpyAsync(&h->scal_host->aux, &h->scal->aux, sizeof(mx), cudaMemcpyDeviceToHost, h->stream));
@@ -437,27 +443,39 @@ int salec_internal_finish_init(salec_gpu *h, double damp_time_in, double *damp_t
     const double dt2 = local * 2.0;
     h->rp.damp_time = dmax(dt2, damp_time_in);
     if (damp_time_out) *damp_time_out = h->rp.damp_time;
-    k_init_vertex_velocity<<<gv, blk, 0, h->stream>>>(h->ctx());
+    launch_step_kernel(SK_INIT_VERTEX_VELOCITY, h->ctx_t<R>(), h->stream);
     CUDA_TRY(cudaGetLastError());
     for (const char *nm : {"e_vel", "e_ste", "e_dvel"}) {
         int fid = field_by_name(nm);
-        CUDA_TRY(cudaMemsetAsync(field_ptr(h, fid), 0, (size_t)field_ncomp(h, fid) * h->d.PL * sizeof(double), h->stream));
+        CUDA_TRY(cudaMemsetAsync(field_ptr(h, fid), 0, (size_t)field_ncomp(h, fid) * h->d.PL * field_elem(h, fid),
+                                 h->stream));
     }
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return SALEC_OK;
 }
 
+} // namespace
+
+// Last start-up steps on the device (src/salec2d.c:76-94): first EOS call, ghost fills,
+// damping reference state and arrival time, vertex velocities, cleared cell velocities.
+int salec_internal_finish_init(salec_gpu *h, double damp_time_in, double *damp_time_out)
+{
+    return h->mixed ? finish_init_t<float>(h, damp_time_in, damp_time_out)
+                    : finish_init_t<double>(h, damp_time_in, damp_time_out);
+}
+
 int salec_internal_fail(int code, const char *msg) { return fail(code, msg ? msg : "error"); }
 
 // Views of the handle for the output writer (salec_output.cu).
-int salec_internal_field_view(salec_gpu *h, const char *name, const double **base, long long *plane, int *pitch,
-                              int *nx, int *ny, int *nc)
+int salec_internal_field_view(salec_gpu *h, const char *name, const void **base, int *f32, long long *plane,
+                              int *pitch, int *nx, int *ny, int *nc)
 {
     const int fid = field_by_name(name);
     if (fid < 0) return fail(SALEC_ERR_ARG, std::string("unknown field ") + name);
     field_points(h, fid, *nx, *ny);
     *nc = field_ncomp(h, fid);
     *base = field_ptr(h, fid);
+    *f32 = field_f32(h, fid) ? 1 : 0;
     *plane = kFields[fid].loc == L_COL ? 0 : h->d.PL;
     *pitch = h->d.P;
     return SALEC_OK;
@@ -523,6 +541,8 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
     if (run->damp_type < 0 || run->damp_type > 5) return fail(SALEC_ERR_ARG, "unknown damping type");
     if (run->damp_type == SALEC_DAMP_PML3)
         return fail(SALEC_ERR_UNSUPPORTED, "damping = pml3 (advect_flux_pml3) is not supported yet");
+    if (run->precision != SALEC_PRECISION_FP64 && run->precision != SALEC_PRECISION_MIXED)
+        return fail(SALEC_ERR_ARG, "precision must be SALEC_PRECISION_FP64 or SALEC_PRECISION_MIXED");
     salec_gpu *h = new salec_gpu();
     Dims &d = h->d;
     d.nmat = run->nmat;
@@ -552,19 +572,21 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(SALEC_ERR_CUDA, "cudaStreamCreate failed"));
 
-    // one pool, every component plane 256-byte aligned
-    size_t planes = 0;
-    for (int k = 0; k < kNumFields; ++k) planes += kFields[k].loc == L_COL ? 0 : (size_t)field_ncomp(h, k);
+    // one pool, every component plane 128-byte aligned (PL is a multiple of 32 elements)
+    h->mixed = run->precision == SALEC_PRECISION_MIXED ? 1 : 0;
     const size_t col = (((size_t)d.enx + 31) / 32) * 32;
-    h->pool_doubles = planes * (size_t)d.PL + col;
-    if (cudaMalloc(&h->pool, h->pool_doubles * sizeof(double)) != cudaSuccess)
-        return bail(fail(SALEC_ERR_ALLOC, "device pool of " + std::to_string(h->pool_doubles * 8) + " bytes"));
-    if (cudaMemsetAsync(h->pool, 0, h->pool_doubles * sizeof(double), h->stream) != cudaSuccess)
+    size_t bytes = 0;
+    for (int k = 0; k < kNumFields; ++k)
+        bytes += kFields[k].loc == L_COL ? col * sizeof(double) : (size_t)field_ncomp(h, k) * d.PL * field_elem(h, k);
+    h->pool_bytes = bytes;
+    if (cudaMalloc(&h->pool, h->pool_bytes) != cudaSuccess)
+        return bail(fail(SALEC_ERR_ALLOC, "device pool of " + std::to_string(h->pool_bytes) + " bytes"));
+    if (cudaMemsetAsync(h->pool, 0, h->pool_bytes, h->stream) != cudaSuccess)
         return bail(fail(SALEC_ERR_CUDA, "pool memset failed"));
     size_t off = 0;
     for (int k = 0; k < kNumFields; ++k) {
-        field_ptr(h, k) = h->pool + off;
-        off += kFields[k].loc == L_COL ? col : (size_t)field_ncomp(h, k) * d.PL;
+        field_ptr(h, k) = reinterpret_cast<double *>(h->pool + off);
+        off += kFields[k].loc == L_COL ? col * sizeof(double) : (size_t)field_ncomp(h, k) * d.PL * field_elem(h, k);
     }
 
     std::vector<DevMat> dms(d.nmat);
@@ -828,7 +850,7 @@ int salec_gpu_check(salec_gpu *h, long long *n_bad)
     for (const char *nm : names) {
         int fid = field_by_name(nm);
         const long long n = (long long)field_ncomp(h, fid) * h->d.PL;
-        k_count_nonfinite<<<592, 256, 0, h->stream>>>(field_ptr(h, fid), n, cnt);
+        launch_count_nonfinite(field_ptr(h, fid), field_f32(h, fid), n, cnt, h->stream);
     }
     CUDA_TRY(cudaGetLastError());
     unsigned long long bad = 0;

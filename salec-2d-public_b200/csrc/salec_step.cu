@@ -18,20 +18,24 @@ namespace salec {
 #define KIDX(i, j) ((long long)(i) + (long long)c.d.P * (long long)(j))
 #define PLN(ptr, comp) ((ptr) + (long long)(comp) * c.d.PL)
 
-__device__ __forceinline__ bool cell_interior(const Ctx &c, int i, int j)
+template <class C>
+__device__ __forceinline__ bool cell_interior(const C &c, int i, int j)
 {
     return i >= 2 && i <= c.d.enx - 3 && j >= 2 && j <= c.d.eny - 3;
 }
-__device__ __forceinline__ bool vert_active(const Ctx &c, int i, int j)
+template <class C>
+__device__ __forceinline__ bool vert_active(const C &c, int i, int j)
 {
     return i >= 1 && i <= c.d.vnx - 2 && j >= 1 && j <= c.d.vny - 2;
 }
-__device__ __forceinline__ bool vert_pad(const Ctx &c, int i, int j)
+template <class C>
+__device__ __forceinline__ bool vert_pad(const C &c, int i, int j)
 {
     int xd = min(i, c.d.vnx - 1 - i), yd = min(j, c.d.vny - 1 - j);
     return xd <= 1 || yd <= 1;
 }
-__device__ __forceinline__ double step_dt(const Ctx &c)
+template <class C>
+__device__ __forceinline__ double step_dt(const C &c)
 {
     // Min(max_dt, CFL reduction) as in src/salec2d.c:167
     double r = ord_decode(c.scal->dt_acc);
@@ -41,13 +45,15 @@ __device__ __forceinline__ double step_dt(const Ctx &c)
 // ============================================================ phase 0: surface profile
 // trace_profile (src/ejecta.c:8-63): per column, MIN of cell-centre y over cells whose vacuum
 // fraction exceeds 0.1; cells above the ejecta threshold with no vacuum get e_ejt = 1.
-__global__ void k_profile_reset(const Ctx c)
+template <class R>
+__global__ void k_profile_reset(const CtxT<R> c)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < c.d.enx) c.f.y_profile[i] = __longlong_as_double((long long)ord_encode(c.rp.threshold_z * 2.0));
 }
 
-__global__ void k_trace_profile(const Ctx c)
+template <class R>
+__global__ void k_trace_profile(const CtxT<R> c)
 {
     __shared__ unsigned long long smin[8][32];
     const int i = blockIdx.x * 32 + threadIdx.x;
@@ -70,7 +76,8 @@ __global__ void k_trace_profile(const Ctx c)
     }
 }
 
-__global__ void k_profile_decode(const Ctx c)
+template <class R>
+__global__ void k_profile_decode(const CtxT<R> c)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < c.d.enx) {
@@ -81,7 +88,8 @@ __global__ void k_profile_decode(const Ctx c)
 
 // ============================================================ phase 1: vertex volume fractions
 // update_v_vof (src/sale2d.c:751-791): mean of the four surrounding cells.
-__device__ __forceinline__ void vertex_vof(const Ctx &c, int i, int j)
+template <class C>
+__device__ __forceinline__ void vertex_vof(const C &c, int i, int j)
 {
     const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
     const long long p = KIDX(i, j);
@@ -96,13 +104,14 @@ __device__ __forceinline__ void vertex_vof(const Ctx &c, int i, int j)
 // ============================================================ phase 2: vertex momentum
 // update_v_vel_inc (src/sale2d.c:930-1049): add the advected momentum increments of the
 // four cells, weighted by density and corner sub-volume; clamp |v|; count void corners.
-__device__ __forceinline__ void vertex_momentum(const Ctx &c, int i, int j)
+template <class C>
+__device__ __forceinline__ void vertex_momentum(const C &c, int i, int j)
 {
     const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
     const int corner[4] = {2, 3, 0, 1};
     const long long p = KIDX(i, j);
-    double *vx = c.f.v_vel, *vy = PLN(c.f.v_vel, 1);
-    double *m0 = c.f.v_mass, *m1 = PLN(c.f.v_mass, 1);
+    auto *vx = c.f.v_vel, *vy = PLN(c.f.v_vel, 1);
+    auto *m0 = c.f.v_mass, *m1 = PLN(c.f.v_mass, 1);
     const double old_x = vx[p], old_y = vy[p];
     double inc_x = 0., inc_y = 0., vvol = 0., vmass = 0.;
     int void_corner = 0;
@@ -142,7 +151,8 @@ __device__ __forceinline__ void vertex_momentum(const Ctx &c, int i, int j)
 
 // Phases 1 and 2 in one vertex sweep: both read only cell fields that no vertex sweep writes,
 // so one thread per vertex does both (the m_vof and e_dvel/e_den ghost fills run first).
-__global__ void k_vertex_vof_momentum(const Ctx c)
+template <class R>
+__global__ void k_vertex_vof_momentum(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!vert_active(c, i, j)) return;
@@ -152,7 +162,8 @@ __global__ void k_vertex_vof_momentum(const Ctx c)
 
 // ============================================================ phase 3: cell velocity
 // update_e_vel (src/sale2d.c:838-928): mass-weighted mean over the solid corner vertices.
-__global__ void k_cell_velocity(const Ctx c)
+template <class R>
+__global__ void k_cell_velocity(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!cell_interior(c, i, j)) return;
@@ -192,7 +203,8 @@ __global__ void k_cell_velocity(const Ctx c)
 // ============================================================ phase 4: void vertices
 // check_v_vel (src/sale2d.c:1051-1142): a vertex whose four corners are all void takes the
 // density-weighted velocity of its non-empty cells.
-__global__ void k_void_vertices(const Ctx c)
+template <class R>
+__global__ void k_void_vertices(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!vert_active(c, i, j)) return;
@@ -221,7 +233,8 @@ __global__ void k_void_vertices(const Ctx c)
 // ============================================================ phase 5 (+6): velocity gradient,
 // artificial viscosity and the CFL candidate of every interior cell.
 // update_e_gradvel (src/sale2d.c:1144-1236) and calculate_dt (src/sale2d.c:1959-2016).
-__global__ void k_gradient_viscosity_cfl(const Ctx c)
+template <class R>
+__global__ void k_gradient_viscosity_cfl(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     unsigned long long cand = ~0ULL;
@@ -283,15 +296,16 @@ __global__ void k_gradient_viscosity_cfl(const Ctx c)
 }
 
 // phase 6: dt of this cycle (single thread)
-__global__ void k_finalize_dt(const Ctx c)
+template <class R>
+__global__ void k_finalize_dt(const CtxT<R> c)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) c.scal->dt = step_dt(c);
 }
 
 // ============================================================ phase 7: vibration, stress, damage
 // block_vibration (src/strength.c:625-695) and update_e_stress (src/strength.c:7-349).
-template <int NM, bool POR>
-__global__ void __launch_bounds__(256) k_stress(const Ctx c)
+template <class R, int NM, bool POR>
+__global__ void __launch_bounds__(256) k_stress(const CtxT<R> c)
 {
     constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -497,7 +511,8 @@ __global__ void __launch_bounds__(256) k_stress(const Ctx c)
 // calculate_acc_default / calculate_acc_pml (src/velocity.c:9-340): surface integral of
 // pressure + viscosity and deviatoric stress, hoop term, gravity and the nine-point
 // Laplacian damping (ANC); the PML form also integrates the auxiliary v_alpha.
-__global__ void k_vertex_acceleration(const Ctx c)
+template <class R>
+__global__ void k_vertex_acceleration(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!vert_active(c, i, j)) return;
@@ -596,7 +611,8 @@ __global__ void k_vertex_acceleration(const Ctx c)
 
 // ============================================================ phase 9: vertex displacement
 // calculate_v_dis (src/sale2d.c:1238-1268).
-__global__ void k_vertex_displacement(const Ctx c)
+template <class R>
+__global__ void k_vertex_displacement(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!vert_active(c, i, j)) return;
@@ -613,8 +629,8 @@ __global__ void k_vertex_displacement(const Ctx c)
 // ============================================================ phase 10: internal energy
 // update_energy (src/sale2d.c:564-712) with the Wunnemann porosity update. After the vacuum
 // test, every input of the cell is loaded in one batch (no load waits on another).
-template <int NM, bool POR>
-__global__ void __launch_bounds__(256) k_energy(const Ctx c)
+template <class R, int NM, bool POR>
+__global__ void __launch_bounds__(256) k_energy(const CtxT<R> c)
 {
     constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -691,7 +707,8 @@ __device__ __forceinline__ double bilinear4(const double *v, double xi, double e
     return r;
 }
 
-__global__ void k_tracers(const Ctx c)
+template <class R>
+__global__ void k_tracers(const CtxT<R> c)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const Tracers &T = c.tr;
@@ -840,8 +857,8 @@ __device__ __forceinline__ double algebraic_ratio(double vu, double vd, double v
 // Upwind record of one face of cell p (_calculate_flux_set_bphi, src/advect.c:1138-1223): the
 // face is written by the cell it flows out of; a face with zero swept volume gets zero material
 // volumes (see k_flux).
-template <int NM, bool POR, int MM>
-__device__ __forceinline__ void store_face(const Ctx &c, double *f, double vol, const double (&flux)[MM][4], int k,
+template <class R, int NM, bool POR, int MM>
+__device__ __forceinline__ void store_face(const CtxT<R> &c, double *f, double vol, const double (&flux)[MM][4], int k,
                                            long long p, int nmat)
 {
     if (vol > 0.) return;
@@ -874,8 +891,8 @@ __device__ __forceinline__ void store_face(const Ctx &c, double *f, double vol, 
 }
 
 // pass 0: interior cells; pass 1: pad cells (after the ghost fills of m_den, m_eng, ...).
-template <int NM, bool POR>
-__global__ void __launch_bounds__(256) k_flux(const Ctx c, int pass)
+template <class R, int NM, bool POR>
+__global__ void __launch_bounds__(256) k_flux(const CtxT<R> c, int pass)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= c.d.enx || j >= c.d.eny) return;
@@ -895,7 +912,6 @@ __global__ void __launch_bounds__(256) k_flux(const Ctx c, int pass)
     const double rv = swept_volume(px[2], py[2], px[1], py[1], dx[2], dy[2], dx[1], dy[1]);
     const double bv = swept_volume(px[1], py[1], px[0], py[0], dx[1], dy[1], dx[0], dy[0]);
     const double uv = swept_volume(px[3], py[3], px[2], py[2], dx[3], dy[3], dx[2], dy[2]);
-    const double lbru[4] = {lv, bv, rv, uv};
     double vof[MM];
     #pragma unroll
     for (int m = 0; m < nmat; ++m) vof[m] = PLN(c.f.m_vof, m)[p];
@@ -932,7 +948,7 @@ __global__ void __launch_bounds__(256) k_flux(const Ctx c, int pass)
         for (int k = 0; k < 8; ++k) grd[k] = PLN(c.f.e_grad, k)[p];
         double gx = 0., gy = 0.;
         {
-            const double *vv = PLN(c.f.v_vof, prim);
+            const auto *vv = PLN(c.f.v_vof, prim);
             double vq[4];
             #pragma unroll
             for (int k = 0; k < 4; ++k) vq[k] = vv[vl[k]];
@@ -981,7 +997,7 @@ __global__ void __launch_bounds__(256) k_flux(const Ctx c, int pass)
         #pragma unroll
         for (int m = 1; m < nmat; ++m) {
             if (m == prim) continue;
-            const double *vv = PLN(c.f.v_vof, m);
+            const auto *vv = PLN(c.f.v_vof, m);
             double vq[4];
             #pragma unroll
             for (int k = 0; k < 4; ++k) vq[k] = vv[vl[k]];
@@ -1042,10 +1058,10 @@ __global__ void __launch_bounds__(256) k_flux(const Ctx c, int pass)
     }
 
     // faces l, b, r, u
-    store_face<NM, POR>(c, c.f.bx_phi + KIDX(i, j), lv, flux, 0, p, nmat);
-    store_face<NM, POR>(c, c.f.by_phi + KIDX(i, j), bv, flux, 1, p, nmat);
-    store_face<NM, POR>(c, c.f.bx_phi + KIDX(i + 1, j), rv, flux, 2, p, nmat);
-    store_face<NM, POR>(c, c.f.by_phi + KIDX(i, j + 1), uv, flux, 3, p, nmat);
+    store_face<R, NM, POR>(c, c.f.bx_phi + KIDX(i, j), lv, flux, 0, p, nmat);
+    store_face<R, NM, POR>(c, c.f.by_phi + KIDX(i, j), bv, flux, 1, p, nmat);
+    store_face<R, NM, POR>(c, c.f.bx_phi + KIDX(i + 1, j), rv, flux, 2, p, nmat);
+    store_face<R, NM, POR>(c, c.f.by_phi + KIDX(i, j + 1), uv, flux, 3, p, nmat);
 }
 
 // ============================================================ phase 14: remap + damping + EOS
@@ -1061,8 +1077,8 @@ struct CellState {
     double dvx, dvy, st[4], dam, tps, vib, ejt, cvs, eden;
 };
 
-template <int NM, bool POR>
-__device__ __forceinline__ void load_cell(const Ctx &c, long long p, CellState<NM, POR> &s)
+template <class R, int NM, bool POR>
+__device__ __forceinline__ void load_cell(const CtxT<R> &c, long long p, CellState<NM, POR> &s)
 {
     const int nmat = NM > 0 ? NM : c.d.nmat;
     #pragma unroll
@@ -1084,8 +1100,8 @@ __device__ __forceinline__ void load_cell(const Ctx &c, long long p, CellState<N
     s.eden = c.f.e_den[p];
 }
 
-template <int NM, bool POR>
-__device__ __forceinline__ void store_cell(const Ctx &c, long long p, const CellState<NM, POR> &s, bool den)
+template <class R, int NM, bool POR>
+__device__ __forceinline__ void store_cell(const CtxT<R> &c, long long p, const CellState<NM, POR> &s, bool den)
 {
     const int nmat = NM > 0 ? NM : c.d.nmat;
     #pragma unroll
@@ -1110,8 +1126,8 @@ __device__ __forceinline__ void store_cell(const Ctx &c, long long p, const Cell
 // advect_flux_default (src/advect.c:26-302) for one interior cell, into registers. The loads
 // that do not depend on the flow (the cell's own state and the material volumes of its four
 // faces) are all issued before the first dependent one.
-template <int NM, bool POR>
-__device__ __forceinline__ void remap_cell(const Ctx &c, int i, int j, long long p, CellState<NM, POR> &s)
+template <class R, int NM, bool POR>
+__device__ __forceinline__ void remap_cell(const CtxT<R> &c, int i, int j, long long p, CellState<NM, POR> &s)
 {
     constexpr int MM = CellState<NM, POR>::MM;
     const int nmat = NM > 0 ? NM : c.d.nmat;
@@ -1290,8 +1306,8 @@ __device__ __forceinline__ int first_material(const CellState<NM, POR> &s, int n
 
 // damp_on_cell (src/velocity.c:356-767) on the register state; the auxiliary e_alpha is read
 // and written here. Returns whether the cell's state changed.
-template <int NM, bool POR>
-__device__ __forceinline__ bool damp_cell(const Ctx &c, long long p, double dt, CellState<NM, POR> &s)
+template <class R, int NM, bool POR>
+__device__ __forceinline__ bool damp_cell(const CtxT<R> &c, long long p, double dt, CellState<NM, POR> &s)
 {
     const int nmat = NM > 0 ? NM : c.d.nmat;
     const int ty = c.rp.damp_type;
@@ -1399,8 +1415,8 @@ __device__ __forceinline__ bool damp_cell(const Ctx &c, long long p, double dt, 
 }
 
 // ejecta_flow (src/ejecta.c:65-133); launched only when resistance or friction is positive
-template <int NM, bool POR>
-__device__ __forceinline__ void ejecta_drag_cell(const Ctx &c, int i, int j, long long p, double dt,
+template <class R, int NM, bool POR>
+__device__ __forceinline__ void ejecta_drag_cell(const CtxT<R> &c, int i, int j, long long p, double dt,
                                                  CellState<NM, POR> &s)
 {
     const double ey = PLN(c.f.e_pos, 1)[p];
@@ -1422,8 +1438,8 @@ __device__ __forceinline__ void ejecta_drag_cell(const Ctx &c, int i, int j, lon
 }
 
 // update_state (src/sale2d.c:1635-1742) from the register state
-template <int NM, bool POR>
-__device__ __forceinline__ void state_cell(const Ctx &c, long long p, const CellState<NM, POR> &s)
+template <class R, int NM, bool POR>
+__device__ __forceinline__ void state_cell(const CtxT<R> &c, long long p, const CellState<NM, POR> &s)
 {
     constexpr int MM = CellState<NM, POR>::MM;
     const int nmat = NM > 0 ? NM : c.d.nmat;
@@ -1474,8 +1490,8 @@ __device__ __forceinline__ void state_cell(const Ctx &c, long long p, const Cell
 
 // One thread per cell: remap (interior), damping (every cell, while t < damp_time), ejecta
 // drag and EOS (interior). The cell's state is stored once, after damping and drag.
-template <int NM, bool POR>
-__global__ void __launch_bounds__(256) k_remap_damp_state(const Ctx c, int do_remap, int do_damp, int do_ejecta, int do_state)
+template <class R, int NM, bool POR>
+__global__ void __launch_bounds__(256) k_remap_damp_state(const CtxT<R> c, int do_remap, int do_damp, int do_ejecta, int do_state)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= c.d.enx || j >= c.d.eny) return;
@@ -1488,58 +1504,23 @@ __global__ void __launch_bounds__(256) k_remap_damp_state(const Ctx c, int do_re
     const bool state = do_state && interior;
     if (!(remap || damp || ejecta || state)) return;
     CellState<NM, POR> s;
-    if (remap) remap_cell<NM, POR>(c, i, j, p, s);
-    else load_cell<NM, POR>(c, p, s);
+    if (remap) remap_cell<R, NM, POR>(c, i, j, p, s);
+    else load_cell<R, NM, POR>(c, p, s);
     bool dirty = remap;
-    if (damp) dirty |= damp_cell<NM, POR>(c, p, dt, s);
+    if (damp) dirty |= damp_cell<R, NM, POR>(c, p, dt, s);
     if (ejecta) {
-        ejecta_drag_cell<NM, POR>(c, i, j, p, dt, s);
+        ejecta_drag_cell<R, NM, POR>(c, i, j, p, dt, s);
         dirty = true;
     }
-    if (dirty) store_cell<NM, POR>(c, p, s, !state);   // the EOS pass writes e_den itself
-    if (state) state_cell<NM, POR>(c, p, s);
-}
-
-// Launchers: the material count and the porosity switch are template parameters, so that the
-// per-material and per-record arrays of the flux and remap kernels are fully unrolled into
-// registers for the common material counts; other counts use the generic instance.
-#define SALEC_NM_DISPATCH(KERNEL, ...)                                                             \
-    do {                                                                                           \
-        const bool por_ = c.rp.porosity_model != 0;                                                \
-        switch (c.d.nmat) {                                                                        \
-        case 2: if (por_) KERNEL<2, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<2, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
-        case 3: if (por_) KERNEL<3, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<3, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
-        case 4: if (por_) KERNEL<4, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<4, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
-        case 5: if (por_) KERNEL<5, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<5, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
-        default: if (por_) KERNEL<0, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<0, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
-        }                                                                                          \
-    } while (0)
-
-void launch_flux(const Ctx &c, int pass, dim3 g, dim3 b, cudaStream_t s)
-{
-    SALEC_NM_DISPATCH(k_flux, c, pass);
-}
-
-void launch_remap_damp_state(const Ctx &c, int do_remap, int do_damp, int do_ejecta, int do_state, dim3 g, dim3 b,
-                             cudaStream_t s)
-{
-    SALEC_NM_DISPATCH(k_remap_damp_state, c, do_remap, do_damp, do_ejecta, do_state);
-}
-
-void launch_energy(const Ctx &c, dim3 g, dim3 b, cudaStream_t s)
-{
-    SALEC_NM_DISPATCH(k_energy, c);
-}
-
-void launch_stress(const Ctx &c, dim3 g, dim3 b, cudaStream_t s)
-{
-    SALEC_NM_DISPATCH(k_stress, c);
+    if (dirty) store_cell<R, NM, POR>(c, p, s, !state);   // the EOS pass writes e_den itself
+    if (state) state_cell<R, NM, POR>(c, p, s);
 }
 
 // ============================================================ phase 15: cycle control
 // update_cycle_control (src/sale2d.c:71-136): advance time and step counter; seed the next
 // CFL reduction with 1.1 * dt (src/sale2d.c:1961).
-__global__ void k_cycle(const Ctx c)
+template <class R>
+__global__ void k_cycle(const CtxT<R> c)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         Scal *s = c.scal;
@@ -1552,7 +1533,8 @@ __global__ void k_cycle(const Ctx c)
 // ============================================================ initialisation sweeps
 // record_avg_value (src/sale2d.c:1562-1627): reference state of the damping layers and the
 // latest arrival time of the impact wave at a damped cell (MAX over cells).
-__global__ void k_record_reference_state(const Ctx c)
+template <class R>
+__global__ void k_record_reference_state(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     unsigned long long cand = 0ULL;
@@ -1576,7 +1558,8 @@ __global__ void k_record_reference_state(const Ctx c)
 }
 
 // init_v_field (src/sale2d.c:1897-1957): vertex velocity and mass from the cell velocities.
-__global__ void k_init_vertex_velocity(const Ctx c)
+template <class R>
+__global__ void k_init_vertex_velocity(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!vert_active(c, i, j)) return;
@@ -1620,6 +1603,24 @@ __device__ __forceinline__ double apply_op(unsigned op, double v)
     }
 }
 
+template <class T>
+__device__ __forceinline__ void gather_one(const GatherField &gf, int mode, long long d, long long s, unsigned ops,
+                                           double *scratch, long long row)
+{
+    T *base = static_cast<T *>(gf.base);
+    for (int comp = 0; comp < gf.ncomp; ++comp) {
+        T *plane = base + (long long)comp * gf.plane;
+        const unsigned op = (ops >> (3 * comp)) & 7u;
+        if (mode == 0) {
+            plane[d] = (T)apply_op(op, (double)plane[s]);
+        } else if (mode == 1) {
+            scratch[row * gf.ncomp_max + comp] = apply_op(op, (double)plane[s]);
+        } else {
+            plane[d] = (T)scratch[row * gf.ncomp_max + comp];
+        }
+    }
+}
+
 __global__ void k_gather(GatherBatch g, int mode, double *scratch)
 {
     // mode 0: in place; 1: gather into scratch; 2: scatter from scratch
@@ -1629,42 +1630,34 @@ __global__ void k_gather(GatherBatch g, int mode, double *scratch)
     while (f + 1 < g.nfield && t >= g.start[f + 1]) ++f;
     const GatherField &gf = g.field[f];
     const int k = t - g.start[f];
-    const long long d = gf.dst[k], s = gf.src[k];
-    const unsigned ops = gf.ops[k];
-    for (int comp = 0; comp < gf.ncomp; ++comp) {
-        double *plane = gf.base + (long long)comp * gf.plane;
-        const unsigned op = (ops >> (3 * comp)) & 7u;
-        if (mode == 0) {
-            plane[d] = apply_op(op, plane[s]);
-        } else if (mode == 1) {
-            scratch[(long long)t * gf.ncomp_max + comp] = apply_op(op, plane[s]);
-        } else {
-            plane[d] = scratch[(long long)t * gf.ncomp_max + comp];
-        }
-    }
+    if (gf.f32) gather_one<float>(gf, mode, gf.dst[k], gf.src[k], gf.ops[k], scratch, t);
+    else gather_one<double>(gf, mode, gf.dst[k], gf.src[k], gf.ops[k], scratch, t);
 }
 
 // ============================================================ layout conversion
-// Reference AoS block (points x-fastest, components innermost) <-> planes.
-__global__ void k_aos_to_planes(const double *aos, double *base, long long plane, int P, int nx, int ny, int nc)
+// Reference AoS block of doubles (points x-fastest, components innermost) <-> planes of T.
+template <class T>
+__global__ void k_aos_to_planes(const double *aos, T *base, long long plane, int P, int nx, int ny, int nc)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long n = (long long)nx * ny;
     if (t >= n) return;
     const int i = (int)(t % nx), j = (int)(t / nx);
-    for (int k = 0; k < nc; ++k) base[(long long)k * plane + i + (long long)P * j] = aos[t * nc + k];
+    for (int k = 0; k < nc; ++k) base[(long long)k * plane + i + (long long)P * j] = (T)aos[t * nc + k];
 }
 
-__global__ void k_planes_to_aos(const double *base, double *aos, long long plane, int P, int nx, int ny, int nc)
+template <class T>
+__global__ void k_planes_to_aos(const T *base, double *aos, long long plane, int P, int nx, int ny, int nc)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long n = (long long)nx * ny;
     if (t >= n) return;
     const int i = (int)(t % nx), j = (int)(t / nx);
-    for (int k = 0; k < nc; ++k) aos[t * nc + k] = base[(long long)k * plane + i + (long long)P * j];
+    for (int k = 0; k < nc; ++k) aos[t * nc + k] = (double)base[(long long)k * plane + i + (long long)P * j];
 }
 
-__global__ void k_count_nonfinite(const double *base, long long n, unsigned long long *out)
+template <class T>
+__global__ void k_count_nonfinite(const T *base, long long n, unsigned long long *out)
 {
     unsigned long long bad = 0;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
@@ -1672,5 +1665,79 @@ __global__ void k_count_nonfinite(const double *base, long long n, unsigned long
     for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, o);
     if ((threadIdx.x & 31) == 0 && bad) atomicAdd(out, bad);
 }
+
+void launch_aos_to_planes(const double *aos, void *base, bool f32, long long plane, int P, int nx, int ny, int nc,
+                          cudaStream_t s)
+{
+    const int tb = 256;
+    const int nb = (int)(((long long)nx * ny + tb - 1) / tb);
+    if (f32) k_aos_to_planes<float><<<nb, tb, 0, s>>>(aos, static_cast<float *>(base), plane, P, nx, ny, nc);
+    else k_aos_to_planes<double><<<nb, tb, 0, s>>>(aos, static_cast<double *>(base), plane, P, nx, ny, nc);
+}
+
+void launch_planes_to_aos(const void *base, bool f32, double *aos, long long plane, int P, int nx, int ny, int nc,
+                          cudaStream_t s)
+{
+    const int tb = 256;
+    const int nb = (int)(((long long)nx * ny + tb - 1) / tb);
+    if (f32) k_planes_to_aos<float><<<nb, tb, 0, s>>>(static_cast<const float *>(base), aos, plane, P, nx, ny, nc);
+    else k_planes_to_aos<double><<<nb, tb, 0, s>>>(static_cast<const double *>(base), aos, plane, P, nx, ny, nc);
+}
+
+void launch_count_nonfinite(const void *base, bool f32, long long n, unsigned long long *out, cudaStream_t s)
+{
+    if (f32) k_count_nonfinite<float><<<592, 256, 0, s>>>(static_cast<const float *>(base), n, out);
+    else k_count_nonfinite<double><<<592, 256, 0, s>>>(static_cast<const double *>(base), n, out);
+}
+
+// ============================================================ launchers
+// The material count and the porosity switch are template parameters of the flux, remap,
+// energy and stress kernels, so that their per-material arrays unroll into registers for the
+// common material counts; other counts use the generic instance.
+#define SALEC_NM_DISPATCH(KERNEL, ...)                                                                         \
+    do {                                                                                                       \
+        const bool por_ = c.rp.porosity_model != 0;                                                            \
+        switch (c.d.nmat) {                                                                                    \
+        case 2: if (por_) KERNEL<R, 2, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 2, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        case 3: if (por_) KERNEL<R, 3, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 3, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        case 4: if (por_) KERNEL<R, 4, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 4, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        case 5: if (por_) KERNEL<R, 5, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 5, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        default: if (por_) KERNEL<R, 0, true><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 0, false><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        }                                                                                                      \
+    } while (0)
+
+template <class R>
+void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, int a0, int a1, int a2, int a3)
+{
+    const dim3 b(32, 8);
+    const dim3 g((c.d.enx + b.x - 1) / b.x, (c.d.eny + b.y - 1) / b.y);   // cells (and faces)
+    const dim3 gv((c.d.vnx + b.x - 1) / b.x, (c.d.vny + b.y - 1) / b.y);  // vertices
+    const int ncol = (c.d.enx + 255) / 256;
+    switch (k) {
+    case SK_PROFILE_RESET: k_profile_reset<R><<<ncol, 256, 0, s>>>(c); break;
+    case SK_TRACE_PROFILE: k_trace_profile<R><<<dim3((c.d.enx + 31) / 32, (c.d.eny + 63) / 64), b, 0, s>>>(c); break;
+    case SK_PROFILE_DECODE: k_profile_decode<R><<<ncol, 256, 0, s>>>(c); break;
+    case SK_VERTEX_VOF_MOMENTUM: k_vertex_vof_momentum<R><<<gv, b, 0, s>>>(c); break;
+    case SK_CELL_VELOCITY: k_cell_velocity<R><<<g, b, 0, s>>>(c); break;
+    case SK_VOID_VERTICES: k_void_vertices<R><<<gv, b, 0, s>>>(c); break;
+    case SK_GRADIENT: k_gradient_viscosity_cfl<R><<<g, b, 0, s>>>(c); break;
+    case SK_FINALIZE_DT: k_finalize_dt<R><<<1, 32, 0, s>>>(c); break;
+    case SK_STRESS: SALEC_NM_DISPATCH(k_stress, c); break;
+    case SK_ACCELERATION: k_vertex_acceleration<R><<<gv, b, 0, s>>>(c); break;
+    case SK_DISPLACEMENT: k_vertex_displacement<R><<<gv, b, 0, s>>>(c); break;
+    case SK_ENERGY: SALEC_NM_DISPATCH(k_energy, c); break;
+    case SK_TRACERS:
+        if (c.tr.n > 0) k_tracers<R><<<(c.tr.n + 127) / 128, 128, 0, s>>>(c);
+        break;
+    case SK_FLUX: SALEC_NM_DISPATCH(k_flux, c, a0); break;
+    case SK_REMAP_DAMP_STATE: SALEC_NM_DISPATCH(k_remap_damp_state, c, a0, a1, a2, a3); break;
+    case SK_CYCLE: k_cycle<R><<<1, 32, 0, s>>>(c); break;
+    case SK_RECORD_REFERENCE: k_record_reference_state<R><<<g, b, 0, s>>>(c); break;
+    case SK_INIT_VERTEX_VELOCITY: k_init_vertex_velocity<R><<<gv, b, 0, s>>>(c); break;
+    }
+}
+
+template void launch_step_kernel<double>(StepKernel, const CtxT<double> &, cudaStream_t, int, int, int, int);
+template void launch_step_kernel<float>(StepKernel, const CtxT<float> &, cudaStream_t, int, int, int, int);
 
 } // namespace salec

@@ -36,7 +36,10 @@ class RunDesc(ctypes.Structure):
                 ("alpha_damp_x", c_d), ("alpha_damp_y", c_d), ("damp_time", c_d),
                 ("threshold_z", c_d), ("flow_resistance", c_d), ("flow_friction", c_d),
                 ("tracer_lub_y0", c_d), ("tracer_lub_frac", c_d),
-                ("max_dt", c_d), ("dt", c_d), ("time", c_d), ("i_step", c_i)]
+                ("max_dt", c_d), ("dt", c_d), ("time", c_d), ("i_step", c_i), ("precision", c_i)]
+
+PRECISION_FP64 = 0    # salec_precision: plain FP64 (bit-parity form)
+PRECISION_MIXED = 1   # FP32 storage of the relaxed fields, FP64 arithmetic and conserved fields
 
 
 MAT_DOUBLES = ["VaporDen", "MeltDen", "GaCoef", "Yint0", "Yfricint", "Ylimint", "Ydam0", "Yfricdam", "Ylimdam",
@@ -91,6 +94,7 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_output_wait": ([vp], c_i),
             "salec_gpu_func_index": ([ctypes.c_char_p], c_i),
             "salec_gpu_create_from_deck": ([ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(vp)], c_i),
+            "salec_gpu_create_from_deck_ex": ([ctypes.c_char_p, ctypes.c_char_p, c_i, ctypes.POINTER(vp)], c_i),
             "salec_gpu_get_run": ([vp, ctypes.POINTER(RunDesc)], c_i),
             "salec_gpu_stream": ([vp, ctypes.POINTER(vp)], c_i),
             "salec_gpu_profile": ([vp, c_i], c_i),
@@ -179,12 +183,12 @@ class Simulation:
     """One device-resident simulation (a salec_gpu handle)."""
 
     @classmethod
-    def from_deck(cls, deck: str, eos_dir: str) -> "Simulation":
+    def from_deck(cls, deck: str, eos_dir: str, precision: int = PRECISION_FP64) -> "Simulation":
         """Create a simulation from a reference input deck and its EOS folder (no reference code)."""
         self = cls.__new__(cls)
         self._keep = []
         h = ctypes.c_void_p()
-        _check(lib().salec_gpu_create_from_deck(deck.encode(), eos_dir.encode(), ctypes.byref(h)),
+        _check(lib().salec_gpu_create_from_deck_ex(deck.encode(), eos_dir.encode(), int(precision), ctypes.byref(h)),
                "salec_gpu_create_from_deck")
         self.h = h
         self.run = self.get_run()

@@ -57,7 +57,7 @@ def trajectories(kinds: List[str], nsteps: int, root: str, phase_steps: int = 0)
         return {k: f.result() for k, f in futs.items()}
 
 
-def simulation_from_record(rec: Dict):
+def simulation_from_record(rec: Dict, precision: int = 0):
     run = bridge.capi.RunDesc()
     for n, v in rec["run"].items():
         if n == "go":
@@ -65,6 +65,7 @@ def simulation_from_record(rec: Dict):
                 run.go[k] = int(v[k])
         else:
             setattr(run, n, v)
+    run.precision = precision
     sim = bridge.capi.Simulation(run, rec["mats"])
     for n, a in rec["init"].items():
         sim.set_field(n, a)
