@@ -57,7 +57,7 @@ struct DevMat {
 // Run parameters fixed for the whole run (sale2d_var / mesh2d_info members).
 struct RunParams {
     int damp_type, partpres, porosity_model, acoustic_fluid, tensile_failure;
-    int tracer_lubrication;
+    int tracer_lubrication, tracer_lub_gy0, tracer_lub_gy1;
     double avis1, avis2, anc;
     double density_cutoff, velocity_max, velocity_min, acceleration_min;
     double alpha_damp_x, alpha_damp_y, damp_time;

@@ -207,6 +207,7 @@ struct Setup {
     int go[4] = {0, 0, 0, 0};
     int tensile_failure = 0, tracer_lubrication = 0;
     double tracer_lub_y0 = 0, tracer_lub_frac = 0;
+    int tracer_lub_gy0 = 0, tracer_lub_gy1 = 0;   // rows of lubricating tracers (set with the mesh)
     // cycle
     double time0 = 0, time1 = 100, max_dt = 1, dt0 = 0;
     // projectile
@@ -1124,6 +1125,23 @@ int build_host_state(const Setup &S0, Setup &S, HostState &H, std::vector<double
     for (x0i = 0; x0i < ncx + 1; ++x0i)
         if (SX(x0i) >= Lx * S.ox) break;
     const double x0 = -SX(x0i + pad) * S.dx;
+    // rows of the lubricating tracer layer: from tracer.lubrication cells below the surface up to
+    // the surface (src/construct.c:75-91)
+    if (S.tracer_lubrication >= 1) {
+        S.tracer_lub_gy0 = 0;
+        S.tracer_lub_gy1 = ncy;
+        int j = 0;
+        for (; j < ncy + 1; ++j) {
+            const double tmpy = SY(j) * S.dy + y0;
+            S.tracer_lub_gy0 = j;
+            if (tmpy >= S.tracer_lubrication * S.dy * (-1.0)) break;
+        }
+        for (; j < ncy + 1; ++j) {
+            const double tmpy = SY(j) * S.dy + y0;
+            S.tracer_lub_gy1 = j;
+            if (tmpy >= 0.0) break;
+        }
+    }
     std::vector<double> &vpos = H.get("v_pos", NV * 2);
     for (int j = 0; j < vny; ++j)
         for (int i = 0; i < vnx; ++i) {
@@ -1516,7 +1534,6 @@ extern "C" int salec_gpu_create_from_deck_ex(const char *deck_path, const char *
     if (!D.load(deck_path, false, err)) return salec_internal_fail(SALEC_ERR_ARG, err.c_str());
     Setup S0, S;
     if (!load_setup(S0, D, eos_dir, err)) return salec_internal_fail(SALEC_ERR_ARG, err.c_str());
-    if (S0.damp_type == 2) return salec_internal_fail(SALEC_ERR_UNSUPPORTED, "damping = pml3 is not supported yet");
     HostState H;
     std::vector<double> tracer_rows;
     int rc = build_host_state(S0, S, H, tracer_rows, err);
@@ -1549,6 +1566,8 @@ extern "C" int salec_gpu_create_from_deck_ex(const char *deck_path, const char *
     run.flow_resistance = S.ejecta_resistance;
     run.flow_friction = S.ejecta_friction;
     run.tracer_lub_y0 = S.tracer_lub_y0;
+    run.tracer_lub_gy0 = S.tracer_lub_gy0;
+    run.tracer_lub_gy1 = S.tracer_lub_gy1;
     run.tracer_lub_frac = S.tracer_lub_frac;
     run.max_dt = S.max_dt;
     run.dt = S.dt0;

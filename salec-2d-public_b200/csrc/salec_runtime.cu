@@ -133,6 +133,10 @@ struct salec_gpu {
     std::vector<int> ev_phase;
     size_t ev_used = 0;
     long long launches = 0;     // kernels launched by this handle
+    // one full cycle captured as a CUDA graph (kernel arguments hold the run parameters and the
+    // tracer arrays, so changing either drops the graph)
+    cudaGraphExec_t cycle_graph = nullptr;
+    long long cycle_graph_launches = 0;
     void *output = nullptr;     // output writer state (salec_output.cu)
 
     template <class R>
@@ -282,7 +286,14 @@ int run_phase_t(salec_gpu *h, int ph)
         rc = run_gather(h, h->g_flux_state);
         launch_step_kernel(SK_FLUX, c, s, 1);
         break;
-    case 13: break;   // strength condition from tracers (lubrication is rejected at create)
+    case 13:   // strength condition: count the lubricating tracers of every cell in e_cnd
+        if (h->rp.tracer_lubrication > 0) {
+            const int fid = field_by_name("e_cnd");
+            CUDA_TRY(cudaMemsetAsync(field_ptr(h, fid), 0, (size_t)h->d.PL * field_elem(h, fid), s));
+            launch_step_kernel(SK_STRENGTH_CONDITION, c, s);
+            if (h->tr.n > 0) h->launches += 1;
+        }
+        break;
     case 14: {
         const int ejecta = (h->rp.flow_resistance > 0. || h->rp.flow_friction > 0.) ? 1 : 0;
         launch_step_kernel(SK_REMAP_DAMP_STATE, c, s, 1, 1, ejecta, 1);
@@ -419,6 +430,7 @@ void release(salec_gpu *h)
     if (h->scal_host) cudaFreeHost(h->scal_host);
     if (h->mat) cudaFree(h->mat);
     if (h->tr_block) cudaFree(h->tr_block);
+    if (h->cycle_graph) cudaGraphExecDestroy(h->cycle_graph);
     for (auto e : h->ev_a) cudaEventDestroy(e);
     for (auto e : h->ev_b) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -536,11 +548,7 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
     *out = nullptr;
     if (run->nx < 4 || run->ny < 4) return fail(SALEC_ERR_ARG, "mesh must have at least 4x4 cells");
     if (run->nmat < 2 || run->nmat > SALEC_MAXMAT) return fail(SALEC_ERR_ARG, "nmat must be in [2, 10]");
-    if (run->tracer_lubrication > 0)
-        return fail(SALEC_ERR_UNSUPPORTED, "tracer lubrication (tracer.lubrication > 0) is not supported");
     if (run->damp_type < 0 || run->damp_type > 5) return fail(SALEC_ERR_ARG, "unknown damping type");
-    if (run->damp_type == SALEC_DAMP_PML3)
-        return fail(SALEC_ERR_UNSUPPORTED, "damping = pml3 (advect_flux_pml3) is not supported yet");
     if (run->precision != SALEC_PRECISION_FP64 && run->precision != SALEC_PRECISION_MIXED)
         return fail(SALEC_ERR_ARG, "precision must be SALEC_PRECISION_FP64 or SALEC_PRECISION_MIXED");
     salec_gpu *h = new salec_gpu();
@@ -560,6 +568,8 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
     rp.damp_type = run->damp_type; rp.partpres = run->partpres; rp.porosity_model = run->porosity_model;
     rp.acoustic_fluid = run->acoustic_fluid; rp.tensile_failure = run->tensile_failure;
     rp.tracer_lubrication = run->tracer_lubrication;
+    rp.tracer_lub_gy0 = run->tracer_lub_gy0;
+    rp.tracer_lub_gy1 = run->tracer_lub_gy1;
     rp.avis1 = run->avis1; rp.avis2 = run->avis2; rp.anc = run->anc;
     rp.density_cutoff = run->density_cutoff; rp.velocity_max = run->velocity_max;
     rp.velocity_min = run->velocity_min; rp.acceleration_min = run->acceleration_min;
@@ -675,13 +685,66 @@ int salec_gpu_phases(salec_gpu *h, int first, int last)
     return SALEC_OK;
 }
 
+namespace {
+
+void drop_cycle_graph(salec_gpu *h)
+{
+    if (h->cycle_graph) cudaGraphExecDestroy(h->cycle_graph);
+    h->cycle_graph = nullptr;
+}
+
+// Capture phases 0-15 of one cycle on the handle's stream into a graph; on any failure the
+// cycle is simply launched kernel by kernel.
+void capture_cycle_graph(salec_gpu *h)
+{
+    cudaGraph_t g = nullptr;
+    const long long before = h->launches;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    int rc = SALEC_OK;
+    for (int p = 0; p <= 15 && rc == SALEC_OK; ++p) rc = run_phase(h, p);
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->launches = before;
+    if (rc != SALEC_OK || e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return;
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (cudaGraphInstantiate(&exec, g, 0) == cudaSuccess) {
+        h->cycle_graph = exec;
+        size_t n = 0;
+        cudaGraphGetNodes(g, nullptr, &n);
+        std::vector<cudaGraphNode_t> nodes(n);
+        long long kernels = 0;
+        if (n && cudaGraphGetNodes(g, nodes.data(), &n) == cudaSuccess)
+            for (size_t k = 0; k < n; ++k) {
+                cudaGraphNodeType ty;
+                if (cudaGraphNodeGetType(nodes[k], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) ++kernels;
+            }
+        h->cycle_graph_launches = kernels;
+    }
+    cudaGraphDestroy(g);
+    cudaGetLastError();
+}
+
+} // namespace
+
 int salec_gpu_step(salec_gpu *h, int nsteps)
 {
     if (!h) return fail(SALEC_ERR_ARG, "null handle");
     if (nsteps < 0) return fail(SALEC_ERR_ARG, "negative step count");
+    if (!h->profiling && nsteps > 0 && !h->cycle_graph) capture_cycle_graph(h);
     for (int k = 0; k < nsteps; ++k) {
-        int rc = salec_gpu_phases(h, 0, 15);
-        if (rc) return rc;
+        if (!h->profiling && h->cycle_graph) {
+            CUDA_TRY(cudaGraphLaunch(h->cycle_graph, h->stream));
+            h->launches += h->cycle_graph_launches;
+        } else {
+            int rc = salec_gpu_phases(h, 0, 15);
+            if (rc) return rc;
+        }
     }
     return SALEC_OK;
 }
@@ -743,8 +806,8 @@ int salec_gpu_get_scalar(salec_gpu *h, const char *name, double *value)
 int salec_gpu_set_scalar(salec_gpu *h, const char *name, double value)
 {
     if (!h || !name) return fail(SALEC_ERR_ARG, "null argument");
-    if (!strcmp(name, "damp_time")) { h->rp.damp_time = value; return SALEC_OK; }
-    if (!strcmp(name, "max_dt")) { h->rp.max_dt = value; return SALEC_OK; }
+    if (!strcmp(name, "damp_time")) { h->rp.damp_time = value; drop_cycle_graph(h); return SALEC_OK; }
+    if (!strcmp(name, "max_dt")) { h->rp.max_dt = value; drop_cycle_graph(h); return SALEC_OK; }
     CUDA_TRY(cudaMemcpyAsync(h->scal_host, h->scal, sizeof(Scal), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     Scal s = *h->scal_host;
@@ -762,6 +825,7 @@ int salec_gpu_set_tracers(salec_gpu *h, int n, const double *rows)
 {
     if (!h || n < 0 || (n > 0 && !rows)) return fail(SALEC_ERR_ARG, "bad argument");
     CUDA_TRY(cudaStreamSynchronize(h->stream));
+    drop_cycle_graph(h);
     if (h->tr_block) cudaFree(h->tr_block);
     h->tr_block = nullptr;
     h->tr = Tracers();

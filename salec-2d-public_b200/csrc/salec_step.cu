@@ -769,6 +769,21 @@ __global__ void k_tracers(const CtxT<R> c)
     if (!(nk >= 2 && nk <= c.d.enx - 3 && nj >= 2 && nj <= c.d.eny - 3)) T.alive[t] = 0;
 }
 
+// ============================================================ phase 13: strength condition
+// update_strength_condition (src/strength.c:351-376): e_cnd (cleared before the launch) counts
+// the live tracers of the lubricating rows gy0 <= gy < gy1 in every cell. The counts are small
+// integers, so the order of the atomic additions does not change them.
+template <class R>
+__global__ void k_strength_condition(const CtxT<R> c)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const Tracers &T = c.tr;
+    if (t >= T.n || !T.alive[t]) return;
+    const int gy = T.gy[t];
+    if (gy < c.rp.tracer_lub_gy1 && gy >= c.rp.tracer_lub_gy0)
+        atomicAdd(c.f.e_cnd + KIDX(T.cx[t], T.cy[t]), (R)1.0);
+}
+
 // ============================================================ phase 12: face flux volumes
 // calculate_flux_mixed (src/advect.c:861-1136) with _calculate_flux_set_bphi (:1138-1223):
 // swept face volumes, geometric cut-line reconstruction of the primary material, algebraic
@@ -1126,7 +1141,7 @@ __device__ __forceinline__ void store_cell(const CtxT<R> &c, long long p, const 
 // advect_flux_default (src/advect.c:26-302) for one interior cell, into registers. The loads
 // that do not depend on the flow (the cell's own state and the material volumes of its four
 // faces) are all issued before the first dependent one.
-template <class R, int NM, bool POR>
+template <class R, int NM, bool POR, bool P3>
 __device__ __forceinline__ void remap_cell(const CtxT<R> &c, int i, int j, long long p, CellState<NM, POR> &s)
 {
     constexpr int MM = CellState<NM, POR>::MM;
@@ -1158,6 +1173,23 @@ __device__ __forceinline__ void remap_cell(const CtxT<R> &c, int i, int j, long 
     const double dam0 = c.f.e_dam[p], tps0 = c.f.e_tps[p], vib0 = c.f.e_vib[p], ejt0 = c.f.e_ejt[p];
     const double cvs0 = por ? c.f.e_cvs[p] : 0.0;
 
+    // advect_flux_pml3 (src/advect.c:304-594) differs from the default remap in the PML
+    // auxiliaries e_beta (fluxes of mass, energy and momentum weighted by the layer's sigma,
+    // accumulated here and damped below), in its clamps and low-density test, and in leaving the
+    // porosity state alone
+    constexpr bool p3 = P3;   // damping = pml3
+    double sgx = 0., sgy = 0., eb0 = 0., eb1 = 0., eb2 = 0., eb3 = 0.;
+    if (p3) {
+        sgx = c.f.e_sigma[p];
+        sgy = PLN(c.f.e_sigma, 1)[p];
+        eb0 = c.f.e_beta[p];
+        eb1 = PLN(c.f.e_beta, 1)[p];
+        eb2 = PLN(c.f.e_beta, 2)[p];
+        eb3 = PLN(c.f.e_beta, 3)[p];
+    }
+    const bool p3_layer = p3 && (sgx > 0. || sgy > 0.);
+    const double para[4] = {-sgy, -sgx, -sgy, -sgx};   // faces l, b, r, u
+
     double dphi[4 * MM + 11];
     #pragma unroll
     for (int q = 0; q < phi; ++q) dphi[q] = 0.;
@@ -1168,7 +1200,7 @@ __device__ __forceinline__ void remap_cell(const CtxT<R> &c, int i, int j, long 
         #pragma unroll
         for (int m = 0; m < nmat; ++m) {
             const double mv = dir[k] * fv[k][m];
-            if (mv == 0.0) continue;   // adds only signed zeros to dphi (see k_flux)
+            if (mv == 0.0) continue;   // adds only signed zeros to dphi and e_beta (see k_flux)
             const double rho_f = f[(m + nmat) * PL];
             dphi[m] += mv;
             dphi[m + nmat] += mv * rho_f;
@@ -1176,9 +1208,15 @@ __device__ __forceinline__ void remap_cell(const CtxT<R> &c, int i, int j, long 
             const double fm = mv * rho_f;
             #pragma unroll
             for (int q = 0; q < 10; ++q) dphi[b + q] += fm * f[(b + q) * PL];
-            if (por) {
+            if (por && !p3) {
                 dphi[b + 10] += (f[(b + 10) * PL]) * (mv * rho_f);
                 dphi[m + b + 11] += (f[(m + b + 11) * PL]) * (mv * rho_f);
+            }
+            if (p3_layer) {
+                eb0 += mv * rho_f * para[k];
+                eb1 += mv * f[(m + 2 * nmat) * PL] * para[k];
+                eb2 += mv * rho_f * para[k] * f[b * PL];
+                eb3 += mv * rho_f * para[k] * f[(b + 1) * PL];
             }
         }
     }
@@ -1200,16 +1238,44 @@ __device__ __forceinline__ void remap_cell(const CtxT<R> &c, int i, int j, long 
     sphi[b + 7] = emass * tps0 + 1.0 * dphi[b + 7];
     sphi[b + 8] = emass * vib0 + 1.0 * dphi[b + 8];
     sphi[b + 9] = emass * ejt0 + 1.0 * dphi[b + 9];
-    if (por) {
+    if (por && !p3) {
         sphi[b + 10] = emass * cvs0 + 1.0 * dphi[b + 10];
         #pragma unroll
         for (int m = 0; m < nmat; ++m) sphi[b + 11 + m] = vof[m] * evol * rho[m] * pty[m] + 1.0 * dphi[b + 11 + m];
+    }
+    if (p3 && sgx + sgy > 0.) {
+        const double adxy = c.rp.alpha_damp_x + c.rp.alpha_damp_y;
+        const double dt = c.scal->dt;
+        eb0 += -1.0 * adxy * eb0 * dt;
+        eb1 += -1.0 * adxy * eb1 * dt;
+        eb2 += -1.0 * adxy * eb2 * dt;
+        eb3 += -1.0 * adxy * eb3 * dt;
+        if (sphi[0] < SALEC_TOLVOF) {
+            sphi[b] += eb2 * dt;
+            sphi[b + 1] += eb3 * dt;
+        }
+        int mf = -1;   // first material (from 1) with a positive volume
+        #pragma unroll
+        for (int m = (NM > 0 ? NM : SALEC_MAXMAT) - 1; m >= 1; --m)
+            if (m < nmat && sphi[m] > SALEC_TOLVOF) mf = m;
+        #pragma unroll
+        for (int m = 1; m < nmat; ++m)
+            if (m == mf) {
+                sphi[m + nmat] += eb0 * dt;
+                sphi[m + 2 * nmat] += eb1 * dt;
+            }
+    }
+    if (p3_layer) {
+        c.f.e_beta[p] = eb0;
+        PLN(c.f.e_beta, 1)[p] = eb1;
+        PLN(c.f.e_beta, 2)[p] = eb2;
+        PLN(c.f.e_beta, 3)[p] = eb3;
     }
     double zeta = 0.0;
     emass = 0.;
     #pragma unroll
     for (int m = 0; m < nmat; ++m) {
-        if (sphi[m] < 0.) { sphi[m] = 0.; sphi[m + nmat] = 0.; }
+        if (sphi[m] < 0. || (p3 && sphi[m + nmat] < 0.)) { sphi[m] = 0.; sphi[m + nmat] = 0.; }
         if (m == 0) continue;
         zeta += sphi[m];
         emass += sphi[m + nmat];
@@ -1235,13 +1301,13 @@ __device__ __forceinline__ void remap_cell(const CtxT<R> &c, int i, int j, long 
     }
     #pragma unroll
     for (int m = 1; m < nmat; ++m) {
-        if (vof[m] < SALEC_TOLVOF || sphi[m + nmat] < SALEC_TOLRHO * SALEC_TOLVOF * evol) {
+        if (vof[m] < SALEC_TOLVOF || (!p3 && sphi[m + nmat] < SALEC_TOLRHO * SALEC_TOLVOF * evol)) {
             eng[m] = 0.0; rho[m] = 0.0; vof[m] = 0.0;
-            if (por) pty[m] = 1.0;
+            if (por && !p3) pty[m] = 1.0;
         } else {
             eng[m] = sphi[m + 2 * nmat] / (vof[m] * evol);
             rho[m] = sphi[m + nmat] / (vof[m] * evol);
-            if (por) pty[m] = sphi[b + 11 + m] / sphi[m + nmat];
+            if (por && !p3) pty[m] = sphi[b + 11 + m] / sphi[m + nmat];
         }
     }
     double dvx, dvy, st[4], dam, tps, vib, ejt, cvs = cvs0;
@@ -1254,28 +1320,28 @@ __device__ __forceinline__ void remap_cell(const CtxT<R> &c, int i, int j, long 
         tps = sphi[b + 7] / emass;
         vib = sphi[b + 8] / emass;
         ejt = sphi[b + 9] / emass;
-        if (por) cvs = sphi[b + 10] / emass;
+        if (por && !p3) cvs = sphi[b + 10] / emass;
     } else {
         dvx = dvy = 0.;
         st[0] = st[1] = st[2] = st[3] = 0.;
         dam = tps = vib = ejt = 0.;
-        if (por) cvs = 0.;
+        if (por && !p3) cvs = 0.;
     }
     double eden = emass / evol;
     tps = wind(tps, 0.0, 10.0);
     dam = wind(dam, 0.0, 1.0);
     ejt = wind(ejt, 0.0, 1.0);
-    if (por)
+    if (por && !p3)
         #pragma unroll
         for (int m = 1; m < nmat; ++m) pty[m] = wind(pty[m], 1.0, c.mat[m].alphamax2);
-    if (eden < c.rp.density_cutoff || eden < 10.0 * c.rp.density_cutoff * (1.0 - vof[0])) {
+    if (eden < c.rp.density_cutoff || (!p3 && eden < 10.0 * c.rp.density_cutoff * (1.0 - vof[0]))) {
         #pragma unroll
         for (int m = 0; m < nmat; ++m) { vof[m] = 0.; rho[m] = 0.; eng[m] = 0.; }
         vof[0] = 1.0;
         dvx = dvy = 0.;
         st[0] = st[1] = st[2] = st[3] = 0.;
         dam = tps = vib = ejt = 0.;
-        if (por) {
+        if (por && !p3) {
             cvs = 0.;
             #pragma unroll
             for (int m = 1; m < nmat; ++m) pty[m] = 1.0;
@@ -1490,7 +1556,7 @@ __device__ __forceinline__ void state_cell(const CtxT<R> &c, long long p, const 
 
 // One thread per cell: remap (interior), damping (every cell, while t < damp_time), ejecta
 // drag and EOS (interior). The cell's state is stored once, after damping and drag.
-template <class R, int NM, bool POR>
+template <class R, int NM, bool POR, bool P3>
 __global__ void __launch_bounds__(256) k_remap_damp_state(const CtxT<R> c, int do_remap, int do_damp, int do_ejecta, int do_state)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1504,7 +1570,7 @@ __global__ void __launch_bounds__(256) k_remap_damp_state(const CtxT<R> c, int d
     const bool state = do_state && interior;
     if (!(remap || damp || ejecta || state)) return;
     CellState<NM, POR> s;
-    if (remap) remap_cell<R, NM, POR>(c, i, j, p, s);
+    if (remap) remap_cell<R, NM, POR, P3>(c, i, j, p, s);
     else load_cell<R, NM, POR>(c, p, s);
     bool dirty = remap;
     if (damp) dirty |= damp_cell<R, NM, POR>(c, p, dt, s);
@@ -1706,6 +1772,18 @@ void launch_count_nonfinite(const void *base, bool f32, long long n, unsigned lo
         }                                                                                                      \
     } while (0)
 
+#define SALEC_NM_DISPATCH_P3(KERNEL, X, ...)                                                                   \
+    do {                                                                                                       \
+        const bool por_ = c.rp.porosity_model != 0;                                                            \
+        switch (c.d.nmat) {                                                                                    \
+        case 2: if (por_) KERNEL<R, 2, true, X><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 2, false, X><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        case 3: if (por_) KERNEL<R, 3, true, X><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 3, false, X><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        case 4: if (por_) KERNEL<R, 4, true, X><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 4, false, X><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        case 5: if (por_) KERNEL<R, 5, true, X><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 5, false, X><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        default: if (por_) KERNEL<R, 0, true, X><<<g, b, 0, s>>>(__VA_ARGS__); else KERNEL<R, 0, false, X><<<g, b, 0, s>>>(__VA_ARGS__); break; \
+        }                                                                                                      \
+    } while (0)
+
 template <class R>
 void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, int a0, int a1, int a2, int a3)
 {
@@ -1730,7 +1808,14 @@ void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, int a0, 
         if (c.tr.n > 0) k_tracers<R><<<(c.tr.n + 127) / 128, 128, 0, s>>>(c);
         break;
     case SK_FLUX: SALEC_NM_DISPATCH(k_flux, c, a0); break;
-    case SK_REMAP_DAMP_STATE: SALEC_NM_DISPATCH(k_remap_damp_state, c, a0, a1, a2, a3); break;
+    case SK_REMAP_DAMP_STATE:
+        // the pml3 remap is its own instance so that its extra state costs the others no registers
+        if (c.rp.damp_type == 2) SALEC_NM_DISPATCH_P3(k_remap_damp_state, true, c, a0, a1, a2, a3);
+        else SALEC_NM_DISPATCH_P3(k_remap_damp_state, false, c, a0, a1, a2, a3);
+        break;
+    case SK_STRENGTH_CONDITION:
+        if (c.tr.n > 0) k_strength_condition<R><<<(c.tr.n + 127) / 128, 128, 0, s>>>(c);
+        break;
     case SK_CYCLE: k_cycle<R><<<1, 32, 0, s>>>(c); break;
     case SK_RECORD_REFERENCE: k_record_reference_state<R><<<g, b, 0, s>>>(c); break;
     case SK_INIT_VERTEX_VELOCITY: k_init_vertex_velocity<R><<<gv, b, 0, s>>>(c); break;

@@ -28,15 +28,15 @@ UPLOAD_FIELDS = [
     "v_vel", "v_bf", "v_acc", "v_dis", "v_pos", "v_vof", "v_mass", "v_vol", "v_subvol", "v_laplace", "v_suf",
     "v_alpha", "e_vel", "e_div_vel", "e_grad_vel", "e_ste", "e_mu", "e_dvel", "e_pre", "e_tem", "e_den", "e_csd",
     "e_dam", "e_cvs", "m_vof", "m_den", "m_eng", "m_pty", "e_wpt", "e_pos", "e_vol", "e_grad", "e_q",
-    "e_strength", "e_cnd", "e_tps", "e_ste2s", "e_sta2s", "e_alpha", "e_sigma", "e_dampref", "e_vib", "e_ejt",
-    "bx_phi", "by_phi", "bx_normal", "by_normal", "y_profile",
+    "e_strength", "e_cnd", "e_tps", "e_ste2s", "e_sta2s", "e_alpha", "e_beta", "e_sigma", "e_dampref", "e_vib",
+    "e_ejt", "bx_phi", "by_phi", "bx_normal", "by_normal", "y_profile",
 ]
 
 # fields the step evolves (compared after every phase)
 STATE_FIELDS = [
     "v_vel", "v_acc", "v_dis", "v_vof", "v_mass", "v_alpha", "e_vel", "e_div_vel", "e_grad_vel", "e_ste", "e_mu",
     "e_dvel", "e_pre", "e_tem", "e_den", "e_csd", "e_dam", "e_cvs", "m_vof", "m_den", "m_eng", "m_pty", "e_wpt",
-    "e_q", "e_strength", "e_tps", "e_ste2s", "e_sta2s", "e_alpha", "e_vib", "e_ejt", "y_profile",
+    "e_q", "e_strength", "e_tps", "e_ste2s", "e_sta2s", "e_alpha", "e_beta", "e_vib", "e_ejt", "e_cnd", "y_profile",
 ]
 
 DAMP_IDS = {0: "pml", 1: "pml2", 2: "pml3", 3: "sbc", 4: "ctlg", 5: "none"}
@@ -144,6 +144,11 @@ def small_deck(kind: str = "base") -> decks.Deck:
     if kind == "sbc_tensile":
         return decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damping="sbc", damp_x=4, damp_y=4,
                           lambda_x=0.3, lambda_y=0.3, tensile_failure=1, right="outflow", bottom="freeslip")
+    if kind == "pml3":
+        return decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damping="pml3", damp_x=4, damp_y=4)
+    if kind == "lubrication":
+        return decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damp_x=4, damp_y=4, velocity=-9000.0,
+                          extra={"tracer": {"lubrication": "3", "lub_y0": "0.0", "lub_frac": "0.5"}})
     if kind == "porous":
         d = decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damp_x=4, damp_y=4, damping="pml2")
         d.materials = [decks.Material("basalt_", porosity="Wunnemann", alpha0=1.0 / 0.75, alphax=1.1,

@@ -16,7 +16,7 @@ import pytest
 import bridge
 import trajectory as tj
 
-KINDS = ["base", "pml2_acfl", "two_mat", "sieden_projectile", "sbc_tensile", "porous"]
+KINDS = ["base", "pml2_acfl", "two_mat", "sieden_projectile", "sbc_tensile", "porous", "pml3", "lubrication"]
 NSTEPS = 40
 TOL_L2 = 1e-9
 TOL_DT = 1e-12
@@ -69,7 +69,7 @@ def test_step_parity(records, cuda_device, kind):
     sim.close()
 
 
-INIT_KINDS = ["base", "two_mat", "sieden_projectile", "porous", "sbc_tensile"]
+INIT_KINDS = ["base", "two_mat", "sieden_projectile", "porous", "sbc_tensile", "pml3", "lubrication"]
 # fields computed by the host initialiser with the reference's own arithmetic: bit-exact
 INIT_EXACT = ["v_pos", "e_pos", "e_vol", "e_grad", "v_vol", "v_subvol", "v_suf", "e_sigma", "bx_normal",
               "by_normal", "v_bf", "m_vof", "m_pty", "e_wpt", "e_tem", "e_dam"]
