@@ -476,6 +476,59 @@ def run_gpu_arm(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- ensemble mode
+def run_ensemble(args):
+    """--ensemble N: N seeded impacts of uneven size (decks.ensemble_decks), each initialised from
+    its deck by the library (host threads in parallel) and stepped --ens-steps cycles, all members
+    together through salec_gpu_step_many. Reports simulations per hour, whole job (deck
+    initialisation included) and device stepping alone."""
+    import concurrent.futures as cf
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    members = decks.ensemble_decks(args.ensemble, seed=args.ens_seed + rank)
+    tmp = tempfile.mkdtemp(prefix="salec_ens_%d_" % rank)
+    paths = []
+    for k, d in enumerate(members):
+        folder = os.path.join(tmp, "m%04d" % k)
+        paths.append((decks.write_deck(d, folder), folder))
+    prec = capi.PRECISION_MIXED if args.ens_precision == "mixed" else capi.PRECISION_FP64
+    t0 = time.perf_counter()
+
+    def make(pf):
+        torch.cuda.set_device(local)
+        return capi.Simulation.from_deck(pf[0], pf[1], precision=prec)
+
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        sims = list(ex.map(make, paths))
+    torch.cuda.synchronize()
+    init_s = time.perf_counter() - t0
+    cells = [s.run.nx * s.run.ny for s in sims]
+    t1 = time.perf_counter()
+    capi.step_many(sims, args.ens_steps, chunk=args.ens_chunk)
+    for s in sims:
+        s.sync()
+    run_s = time.perf_counter() - t1
+    nbad = sum(s.check() for s in sims)
+    for s in sims:
+        s.close()
+    if rank == 0:
+        n = len(sims) * world
+        line = {"metric": "ensemble sims/h", "value": n / (init_s + run_s) * 3600.0, "unit": "simulations/h",
+                "n_gpus": world, "steps": args.ens_steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if prec == capi.PRECISION_FP64 else "f32 storage / f64 arithmetic",
+                "data": "synthetic",
+                "config": {"workload": "ensemble of %d seeded basalt impacts, grids U[128,1024]^2, 5-20 km/s, CPPR "
+                                       "10-40, cohesion 1-100 MPa, friction 0.6-1.4, PML" % args.ensemble,
+                           "members": len(sims), "cells_total": int(sum(cells)), "cycles_each": args.ens_steps,
+                           "chunk": args.ens_chunk, "seed": args.ens_seed},
+                "init_s": init_s, "run_s": run_s,
+                "device_sims_per_h": n / run_s * 3600.0,
+                "cell_updates_per_s": world * sum(cells) * args.ens_steps / run_s,
+                "nonfinite": int(nbad)}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -487,10 +540,17 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
+    ap.add_argument("--ensemble", type=int, default=0, help="run the ensemble mode with this many members")
+    ap.add_argument("--ens-steps", type=int, default=2000)
+    ap.add_argument("--ens-chunk", type=int, default=32)
+    ap.add_argument("--ens-seed", type=int, default=2024)
+    ap.add_argument("--ens-precision", choices=["fp64", "mixed"], default="mixed")
     args = ap.parse_args()
     if args.warmup < 1:
         args.warmup = 1
-    if args.impl == "reference":
+    if args.ensemble > 0 and args.impl == "ours":
+        run_ensemble(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_gpu_arm(args)

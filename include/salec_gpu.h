@@ -146,6 +146,12 @@ int salec_gpu_get_field(salec_gpu *h, int field, double *host, long long n);
 
 /* Advance nsteps full cycles: the loop body of src/salec2d.c:115-272 without the output point. */
 int salec_gpu_step(salec_gpu *h, int nsteps);
+/* Advance an ensemble of independent simulations (each handle a different deck or mesh size)
+ * by nsteps cycles each. Cycles are queued round-robin, chunk cycles per member at a time, each
+ * member on its own stream, so the kernels of small meshes run side by side on the device.
+ * Every member computes exactly what salec_gpu_step() alone would. The call returns once the
+ * work is queued; salec_gpu_sync() on a member waits for it. chunk <= 0 selects 16. */
+int salec_gpu_step_many(salec_gpu *const *handles, int n, int nsteps, int chunk);
 /* Run phases first..last of one cycle, for stepwise checks and timing. Phases follow the
  * reference's loop body (src/salec2d.c): 0 surface profile, 1 vertex volume fractions and
  * vertex momentum + restriction (one vertex sweep), 2 empty (the reference's second half of

@@ -749,6 +749,24 @@ int salec_gpu_step(salec_gpu *h, int nsteps)
     return SALEC_OK;
 }
 
+int salec_gpu_step_many(salec_gpu *const *handles, int n, int nsteps, int chunk)
+{
+    if (!handles || n < 0 || nsteps < 0) return fail(SALEC_ERR_ARG, "bad argument");
+    for (int k = 0; k < n; ++k)
+        if (!handles[k]) return fail(SALEC_ERR_ARG, "null handle in the ensemble");
+    if (chunk <= 0) chunk = 16;
+    // round-robin: every member gets `chunk` cycles queued on its own stream before the next
+    // member's turn, so the members' kernels overlap on the device
+    for (int done = 0; done < nsteps; done += chunk) {
+        const int k_steps = std::min(chunk, nsteps - done);
+        for (int k = 0; k < n; ++k) {
+            int rc = salec_gpu_step(handles[k], k_steps);
+            if (rc) return rc;
+        }
+    }
+    return SALEC_OK;
+}
+
 int salec_gpu_stream(salec_gpu *h, void **stream)
 {
     if (!h || !stream) return fail(SALEC_ERR_ARG, "null argument");

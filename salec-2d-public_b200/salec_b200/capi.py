@@ -83,6 +83,7 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_set_field": ([vp, c_i, P_D, c_ll], c_i),
             "salec_gpu_get_field": ([vp, c_i, P_D, c_ll], c_i),
             "salec_gpu_step": ([vp, c_i], c_i),
+            "salec_gpu_step_many": ([ctypes.POINTER(vp), c_i, c_i, c_i], c_i),
             "salec_gpu_phases": ([vp, c_i, c_i], c_i),
             "salec_gpu_sync": ([vp], c_i),
             "salec_gpu_get_scalar": ([vp, ctypes.c_char_p, P_D], c_i),
@@ -110,6 +111,13 @@ def lib() -> ctypes.CDLL:
             fn.restype = res
         _lib = L
     return _lib
+
+
+def step_many(sims, nsteps: int, chunk: int = 16) -> None:
+    """Advance an ensemble of Simulations by nsteps cycles each, their kernels overlapping on
+    the device (salec_gpu_step_many); returns once queued, sync() waits."""
+    arr = (ctypes.c_void_p * len(sims))(*[s.h.value for s in sims])
+    _check(lib().salec_gpu_step_many(arr, len(sims), int(nsteps), int(chunk)), "salec_gpu_step_many")
 
 
 class SalecError(RuntimeError):

@@ -401,3 +401,25 @@ def config2_deck(n: int = 2048, maxstep: int = 4999) -> Deck:
                 materials=[granite, ice], target_materials=["granit_"], target_depths=[1.0e7],
                 projectile="ice____", radius_cells=40.0, velocity=-15000.0, gravity=-1.62,
                 damping="pml", damp_x=30, damp_y=30, maxstep=maxstep, dt0=1.0e-4, maxdt=0.05)
+
+
+def ensemble_decks(count: int = 256, seed: int = 2024, nmin: int = 128, nmax: int = 1024) -> List[Deck]:
+    """Seeded ensemble of uneven impacts: grids drawn uniformly between nmin and nmax cells per
+    axis, impactor speed U[5, 20] km/s, CPPR U{10..40}, cohesion log-uniform 1-100 MPa, friction
+    U[0.6, 1.4]; basalt Tillotson target and projectile, 30-layer PML (at most a sixth of the mesh)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nx = int(rng.integers(nmin, nmax + 1))
+        ny = int(rng.integers(nmin, nmax + 1))
+        v = float(rng.uniform(5000.0, 20000.0))
+        cppr = int(rng.integers(10, 41))
+        coh = float(10.0 ** rng.uniform(6.0, 8.0))
+        fri = float(rng.uniform(0.6, 1.4))
+        basalt = Material("basalt_", yint0=coh, yintfri=fri, ydam0=coh * 0.01, ydamfri=fri * 0.5)
+        damp = max(4, min(30, min(nx, ny) // 6))
+        out.append(Deck(npx=nx, npy=ny, dx=50.0, dy=50.0, oy=0.5, materials=[basalt], target_materials=["basalt_"],
+                        target_depths=[1.0e7], projectile="basalt_", radius_cells=float(min(cppr, min(nx, ny) // 5)),
+                        velocity=-v, gravity=-1.62, damping="pml", damp_x=damp, damp_y=damp, maxstep=1999,
+                        dt0=1.0e-4, maxdt=0.05))
+    return out
