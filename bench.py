@@ -68,8 +68,10 @@ def kernel_doubles(ph: int, k: dict, m: int, pml2: bool, damping: bool, porous: 
         d = 2 * C + 7 * (C - Cf) + (8 + m + 9 + 9) * Cf   # sta2s, tps, strength, m-1 vof, den, grad_vel 5,
         #                                                   mu, pre, tem, csd and write 9
         return d + (4 * Cf if acoustic else 0)
-    if ph == 8:    # acceleration: v_subvol 4, v_suf 8, v_vol 4, v_laplace 9, v_vel 2, v_mass, v_bf 2,
-        return 32 * V + 7 * C + ((4 * V + 3 * C) if pml2 else 0)   # v_acc w2 | e_pre, e_q, e_ste 4, e_den
+    if ph == 8:    # acceleration: v_subvol 4, v_suf 8, v_vol 4, v_vel 2, v_mass, v_bf 2, v_acc w2 | e_pre,
+        #            e_q, e_ste 4, e_den; the Laplacian weights (9) only where one is non-zero (Vl), plus
+        #            one mask bit per vertex
+        return 23 * V + 9 * k["Vl"] + V / 64.0 + 7 * C + ((4 * V + 3 * C) if pml2 else 0)
     if ph == 9:    # v_dis: v_vel rw, v_acc | v_dis w
         return 8 * V
     if ph == 10:   # energy: vof0, den everywhere; full cells pre, q, div, grad_vel 5, ste 4, vof/den (m-1),
@@ -332,7 +334,9 @@ def run_gpu_arm(args):
     vof0 = sim.get_field("m_vof")[..., 0][2:-2, 2:-2]
     sig = sim.get_field("e_sigma")[2:-2, 2:-2]
     damping = run.damp_type != 5 and run.damp_time > sim.scalar("time")
+    lap = sim.get_field("v_laplace")
     counts = {"C": cells, "V": (n + 3) * (n + 3), "Cp": (n + 4) * (n + 4),
+              "Vl": int(np.count_nonzero(np.any(lap != 0.0, axis=-1))),
               "Cf": int(np.count_nonzero(vof0 <= 1e-6)), "Cn": int(np.count_nonzero(vof0 < 1.0 - 1e-6)),
               "L": int(np.count_nonzero(((sig[..., 0] > 0) | (sig[..., 1] > 0)) & (vof0 < 1.0 - 1e-6)))}
     ntr = len(sim.get_tracers())

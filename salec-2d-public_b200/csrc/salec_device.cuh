@@ -123,6 +123,8 @@ struct CtxT {
     const DevMat *mat;
     Scal *scal;
     Tracers tr;
+    // one bit per vertex (rows of P/32 words): set where any nine-point Laplacian weight is non-zero
+    const unsigned *lap_mask;
 };
 using Ctx = CtxT<double>;
 

@@ -126,6 +126,7 @@ struct salec_gpu {
     Gather g_mvof, g_dvel_den, g_evel, g_pre_ste_q, g_flux_state, r_vel, r_acc, r_dis, g_init;
     Tracers tr{};
     void *tr_block = nullptr;   // one allocation holding every tracer array
+    unsigned *lap_mask = nullptr;   // vertices with a non-zero Laplacian weight (1 bit each)
     salec_run_desc run{};       // the description the handle was created from
     // optional per-phase timing with CUDA events on the handle's stream
     int profiling = 0;
@@ -149,6 +150,7 @@ struct salec_gpu {
         c.mat = mat;
         c.scal = scal;
         c.tr = tr;
+        c.lap_mask = lap_mask;
         return c;
     }
     Ctx ctx() const { return ctx_t<double>(); }
@@ -409,6 +411,11 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
         CUDA_TRY(cudaMemcpyAsync(h->staging, host, need * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         launch_aos_to_planes(h->staging, base, f32, plane, h->d.P, nx, ny, nc, h->stream);
         CUDA_TRY(cudaGetLastError());
+        if (!strcmp(kFields[fid].name, "v_laplace")) {
+            if (h->mixed) launch_step_kernel(SK_LAPLACE_MASK, h->ctx_t<float>(), h->stream);
+            else launch_step_kernel(SK_LAPLACE_MASK, h->ctx_t<double>(), h->stream);
+            CUDA_TRY(cudaGetLastError());
+        }
         CUDA_TRY(cudaStreamSynchronize(h->stream));
     } else {
         launch_planes_to_aos(base, f32, h->staging, plane, h->d.P, nx, ny, nc, h->stream);
@@ -430,6 +437,7 @@ void release(salec_gpu *h)
     if (h->scal_host) cudaFreeHost(h->scal_host);
     if (h->mat) cudaFree(h->mat);
     if (h->tr_block) cudaFree(h->tr_block);
+    if (h->lap_mask) cudaFree(h->lap_mask);
     if (h->cycle_graph) cudaGraphExecDestroy(h->cycle_graph);
     for (auto e : h->ev_a) cudaEventDestroy(e);
     for (auto e : h->ev_b) cudaEventDestroy(e);
@@ -597,6 +605,14 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
     for (int k = 0; k < kNumFields; ++k) {
         field_ptr(h, k) = reinterpret_cast<double *>(h->pool + off);
         off += kFields[k].loc == L_COL ? col * sizeof(double) : (size_t)field_ncomp(h, k) * d.PL * field_elem(h, k);
+    }
+
+    {
+        const size_t words = (size_t)(d.P / 32) * d.R;
+        if (cudaMalloc(&h->lap_mask, words * sizeof(unsigned)) != cudaSuccess)
+            return bail(fail(SALEC_ERR_ALLOC, "Laplacian mask"));
+        if (cudaMemsetAsync(h->lap_mask, 0, words * sizeof(unsigned), h->stream) != cudaSuccess)
+            return bail(fail(SALEC_ERR_CUDA, "Laplacian mask memset"));
     }
 
     std::vector<DevMat> dms(d.nmat);

@@ -578,7 +578,10 @@ __global__ void k_vertex_acceleration(const CtxT<R> c)
     if (pml) { c.f.v_alpha[p] = alx; PLN(c.f.v_alpha, 1)[p] = aly; }
 
     double ancx = 0., ancy = 0.;
-    if (!vert_pad(c, i, j)) {
+    // where all nine weights are zero (outside the ANC band) the stencil sums to +0 and the term
+    // is +0: the weights are not read there
+    const bool lap = (c.lap_mask[(long long)j * (c.d.P >> 5) + (i >> 5)] >> (i & 31)) & 1u;
+    if (!vert_pad(c, i, j) && lap) {
         double lvx = 0., lvy = 0.;
         int k = 0;
         for (int dj = -1; dj <= 1; ++dj)
@@ -1654,6 +1657,21 @@ __global__ void k_init_vertex_velocity(const CtxT<R> c)
     PLN(c.f.v_vel, 1)[p] = vy;
 }
 
+// Bit mask of the vertices with a non-zero nine-point Laplacian weight; one warp per 32
+// consecutive vertices of a row (the grid spans the padded pitch, so warps are whole).
+template <class R>
+__global__ void k_laplace_mask(const CtxT<R> c, unsigned *mask)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    bool nz = false;
+    if (i < c.d.vnx && j < c.d.vny) {
+        const long long p = KIDX(i, j);
+        for (int k = 0; k < 9; ++k) nz = nz || PLN(c.f.v_laplace, k)[p] != (R)0;
+    }
+    const unsigned word = __ballot_sync(0xffffffffu, nz);
+    if ((threadIdx.x & 31) == 0 && j < c.d.vny) mask[(long long)j * (c.d.P >> 5) + (i >> 5)] = word;
+}
+
 // ============================================================ boundary gathers
 // Apply a precomputed gather map (built on the host from the reference's ghost and
 // restriction tables): dst[k] = op_c(src[k]) per component c. In-place when no source is also
@@ -1812,6 +1830,9 @@ void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, int a0, 
         // the pml3 remap is its own instance so that its extra state costs the others no registers
         if (c.rp.damp_type == 2) SALEC_NM_DISPATCH_P3(k_remap_damp_state, true, c, a0, a1, a2, a3);
         else SALEC_NM_DISPATCH_P3(k_remap_damp_state, false, c, a0, a1, a2, a3);
+        break;
+    case SK_LAPLACE_MASK:
+        k_laplace_mask<R><<<dim3(c.d.P / 32, (c.d.vny + 7) / 8), b, 0, s>>>(c, const_cast<unsigned *>(c.lap_mask));
         break;
     case SK_STRENGTH_CONDITION:
         if (c.tr.n > 0) k_strength_condition<R><<<(c.tr.n + 127) / 128, 128, 0, s>>>(c);
