@@ -57,13 +57,14 @@ def kernel_doubles(ph: int, k: dict, m: int, pml2: bool, damping: bool, porous: 
     if ph == 0:    # trace_profile: vof0, centre y
         return 2 * Cp
     if ph == 1:    # update_v_vof: m_vof (m) -> v_vof (m), and in the same sweep update_v_vel_inc:
-        return m * C + m * V + 7 * C + 11 * V   # e_wpt 4, e_den, e_dvel 2 | v_vol 4, v_vel rw, v_mass r1 w2
+        return m * C + m * V + 7 * C + 7 * V + k["T_v_vol"]   # e_wpt 4, e_den, e_dvel 2 | v_vel rw,
+        #                                                        v_mass r1 w2 | v_vol table
     if ph == 3:    # update_e_vel: e_den, e_wpt 4, e_vel w2 | v_mass 2, v_vel 2
         return 7 * C + 4 * V
     if ph == 4:    # check_v_vel: e_den, e_wpt 4 (fills of void vertices are data-dependent)
         return 5 * C
-    if ph == 5:    # gradvel + q + CFL: e_grad 12, e_pos 3, e_vol, vof0, csd, pre, den, e_vel 2 | v_vel 2;
-        return 29 * C + 2 * V    # writes e_grad_vel 5, e_div_vel, e_q
+    if ph == 5:    # gradvel + q + CFL: e_pos 3, vof0, csd, pre, den, e_vel 2 | v_vel 2; writes e_grad_vel 5,
+        return 16 * C + 2 * V + k["T_e_grad"] + k["T_e_vol"]   # e_div_vel, e_q | e_grad, e_vol tables
     if ph == 7:    # stress: vof0, dam everywhere; vacuum cells write 7 zeros; full cells read ste 4, ste2s,
         d = 2 * C + 7 * (C - Cf) + (8 + m + 9 + 9) * Cf   # sta2s, tps, strength, m-1 vof, den, grad_vel 5,
         #                                                   mu, pre, tem, csd and write 9
@@ -71,7 +72,8 @@ def kernel_doubles(ph: int, k: dict, m: int, pml2: bool, damping: bool, porous: 
     if ph == 8:    # acceleration: v_subvol 4, v_suf 8, v_vol 4, v_vel 2, v_mass, v_bf 2, v_acc w2 | e_pre,
         #            e_q, e_ste 4, e_den; the Laplacian weights (9) only where one is non-zero (Vl), plus
         #            one mask bit per vertex
-        return 23 * V + 9 * k["Vl"] + V / 64.0 + 7 * C + ((4 * V + 3 * C) if pml2 else 0)
+        return (7 * V + 9 * k["Vl"] + V / 64.0 + 7 * C + ((4 * V + 3 * C) if pml2 else 0)
+                + k["T_v_subvol"] + k["T_v_suf"] + k["T_v_vol"])
     if ph == 9:    # v_dis: v_vel rw, v_acc | v_dis w
         return 8 * V
     if ph == 10:   # energy: vof0, den everywhere; full cells pre, q, div, grad_vel 5, ste 4, vof/den (m-1),
@@ -335,8 +337,15 @@ def run_gpu_arm(args):
     sig = sim.get_field("e_sigma")[2:-2, 2:-2]
     damping = run.damp_type != 5 and run.damp_time > sim.scalar("time")
     lap = sim.get_field("v_laplace")
+    # geometry read through tables of distinct rows: each table counts once per launch
+    tables = {}
+    for gname in ("v_vol", "v_subvol", "v_suf", "e_grad", "e_vol"):
+        a = sim.get_field(gname)
+        rows = {a[j].tobytes() for j in range(a.shape[0])}
+        nrow = len(rows) if len(rows) <= 512 and len(rows) < a.shape[0] else a.shape[0]
+        tables["T_" + gname] = float(nrow * a.shape[1] * a.shape[2])
     counts = {"C": cells, "V": (n + 3) * (n + 3), "Cp": (n + 4) * (n + 4),
-              "Vl": int(np.count_nonzero(np.any(lap != 0.0, axis=-1))),
+              "Vl": int(np.count_nonzero(np.any(lap != 0.0, axis=-1))), **tables,
               "Cf": int(np.count_nonzero(vof0 <= 1e-6)), "Cn": int(np.count_nonzero(vof0 < 1.0 - 1e-6)),
               "L": int(np.count_nonzero(((sig[..., 0] > 0) | (sig[..., 1] > 0)) & (vof0 < 1.0 - 1e-6)))}
     ntr = len(sim.get_tracers())

@@ -114,6 +114,16 @@ struct Tracers {
     int n;
 };
 
+// A geometry field read through a table of its distinct rows: mesh row j holds the values of
+// table row row[j] (the identity map over the field's own planes when the rows do not repeat).
+// The values read are the field's own values; only their location differs.
+template <class T>
+struct GeoTab {
+    const T *tab;      // component-0 plane of the table
+    const int *row;    // table row of every mesh row
+    long long plane;   // elements between components
+};
+
 template <class R>
 struct CtxT {
     using real = R;
@@ -125,6 +135,8 @@ struct CtxT {
     Tracers tr;
     // one bit per vertex (rows of P/32 words): set where any nine-point Laplacian weight is non-zero
     const unsigned *lap_mask;
+    GeoTab<R> g_v_vol, g_v_subvol, g_v_suf, g_e_grad;
+    GeoTab<double> g_e_vol;
 };
 using Ctx = CtxT<double>;
 

@@ -13,6 +13,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 using namespace salec;
@@ -127,6 +129,15 @@ struct salec_gpu {
     Tracers tr{};
     void *tr_block = nullptr;   // one allocation holding every tracer array
     unsigned *lap_mask = nullptr;   // vertices with a non-zero Laplacian weight (1 bit each)
+    // geometry fields read through tables of their distinct rows: v_vol, v_subvol, v_suf,
+    // e_grad, e_vol (tab and row are owned when compact)
+    struct GeoSlot {
+        void *tab = nullptr;
+        int *row = nullptr;
+        long long plane = 0;
+        bool compact = false;
+    } geo[5];
+    int *row_identity = nullptr;
     salec_run_desc run{};       // the description the handle was created from
     // optional per-phase timing with CUDA events on the handle's stream
     int profiling = 0;
@@ -151,6 +162,11 @@ struct salec_gpu {
         c.scal = scal;
         c.tr = tr;
         c.lap_mask = lap_mask;
+        c.g_v_vol = {static_cast<const R *>(geo[0].tab), geo[0].row, geo[0].plane};
+        c.g_v_subvol = {static_cast<const R *>(geo[1].tab), geo[1].row, geo[1].plane};
+        c.g_v_suf = {static_cast<const R *>(geo[2].tab), geo[2].row, geo[2].plane};
+        c.g_e_grad = {static_cast<const R *>(geo[3].tab), geo[3].row, geo[3].plane};
+        c.g_e_vol = {static_cast<const double *>(geo[4].tab), geo[4].row, geo[4].plane};
         return c;
     }
     Ctx ctx() const { return ctx_t<double>(); }
@@ -389,6 +405,79 @@ int upload_material(salec_gpu *h, const salec_material_desc &m, DevMat &dm)
     return SALEC_OK;
 }
 
+const char *const kGeoFields[5] = {"v_vol", "v_subvol", "v_suf", "e_grad", "e_vol"};
+constexpr int kGeoMaxRows = 512;   // more distinct rows than this: read the field's own planes
+
+// Table of the distinct rows of an uploaded geometry field (host AoS data `host`, nx x ny
+// points of nc components), compared bit for bit; mesh rows that repeat share one table row.
+int build_geo_table(salec_gpu *h, int slot, int fid, const double *host, int nx, int ny, int nc)
+{
+    auto &g = h->geo[slot];
+    const size_t row_doubles = (size_t)nx * nc;
+    // row hashes on host threads, then the rows grouped in order (equal rows compared in full)
+    std::vector<unsigned long long> hashes(ny);
+    {
+        const int nt = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 16));
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back([&, t]() {
+                for (int j = t; j < ny; j += nt) {
+                    const double *r = host + (size_t)j * row_doubles;
+                    unsigned long long hsh = 1469598103934665603ULL;
+                    for (size_t k = 0; k < row_doubles; ++k) {
+                        unsigned long long w;
+                        memcpy(&w, r + k, sizeof(w));
+                        hsh = (hsh ^ w) * 0x9E3779B97F4A7C15ULL;
+                        hsh ^= hsh >> 29;
+                    }
+                    hashes[j] = hsh;
+                }
+            });
+        for (auto &th : pool) th.join();
+    }
+    std::unordered_map<unsigned long long, std::vector<int>> buckets;
+    std::vector<int> rowmap(h->d.R, 0), uniq;
+    for (int j = 0; j < ny; ++j) {
+        const double *r = host + (size_t)j * row_doubles;
+        const unsigned long long hsh = hashes[j];
+        int found = -1;
+        for (int u : buckets[hsh])
+            if (!memcmp(host + (size_t)uniq[u] * row_doubles, r, row_doubles * sizeof(double))) { found = u; break; }
+        if (found < 0) {
+            found = (int)uniq.size();
+            uniq.push_back(j);
+            buckets[hsh].push_back(found);
+        }
+        rowmap[j] = found;
+    }
+    if (g.compact) { cudaFree(g.tab); cudaFree(g.row); }
+    g = salec_gpu::GeoSlot();
+    if (h->cycle_graph) { cudaGraphExecDestroy(h->cycle_graph); h->cycle_graph = nullptr; }
+    const int U = (int)uniq.size();
+    if (U > kGeoMaxRows || U >= ny) {
+        g.tab = field_ptr(h, fid);
+        g.row = h->row_identity;
+        g.plane = h->d.PL;
+        return SALEC_OK;
+    }
+    const bool f32 = field_f32(h, fid);
+    const long long plane = (((long long)U * h->d.P + 31) / 32) * 32;
+    std::vector<double> compact((size_t)U * row_doubles);
+    for (int u = 0; u < U; ++u)
+        memcpy(&compact[(size_t)u * row_doubles], host + (size_t)uniq[u] * row_doubles, row_doubles * sizeof(double));
+    CUDA_TRY(cudaMalloc(&g.tab, (size_t)nc * plane * field_elem(h, fid)));
+    CUDA_TRY(cudaMalloc(&g.row, sizeof(int) * h->d.R));
+    g.compact = true;
+    g.plane = plane;
+    CUDA_TRY(cudaMemcpyAsync(h->staging, compact.data(), compact.size() * sizeof(double), cudaMemcpyHostToDevice,
+                             h->stream));
+    launch_aos_to_planes(h->staging, g.tab, f32, plane, h->d.P, nx, U, nc, h->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(g.row, rowmap.data(), sizeof(int) * h->d.R, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return SALEC_OK;
+}
+
 int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
 {
     if (fid < 0 || fid >= kNumFields) return fail(SALEC_ERR_ARG, "unknown field");
@@ -411,6 +500,11 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
         CUDA_TRY(cudaMemcpyAsync(h->staging, host, need * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         launch_aos_to_planes(h->staging, base, f32, plane, h->d.P, nx, ny, nc, h->stream);
         CUDA_TRY(cudaGetLastError());
+        for (int k = 0; k < 5; ++k)
+            if (!strcmp(kFields[fid].name, kGeoFields[k])) {
+                int rc = build_geo_table(h, k, fid, host, nx, ny, nc);
+                if (rc) return rc;
+            }
         if (!strcmp(kFields[fid].name, "v_laplace")) {
             if (h->mixed) launch_step_kernel(SK_LAPLACE_MASK, h->ctx_t<float>(), h->stream);
             else launch_step_kernel(SK_LAPLACE_MASK, h->ctx_t<double>(), h->stream);
@@ -438,6 +532,9 @@ void release(salec_gpu *h)
     if (h->mat) cudaFree(h->mat);
     if (h->tr_block) cudaFree(h->tr_block);
     if (h->lap_mask) cudaFree(h->lap_mask);
+    for (auto &g : h->geo)
+        if (g.compact) { cudaFree(g.tab); cudaFree(g.row); }
+    if (h->row_identity) cudaFree(h->row_identity);
     if (h->cycle_graph) cudaGraphExecDestroy(h->cycle_graph);
     for (auto e : h->ev_a) cudaEventDestroy(e);
     for (auto e : h->ev_b) cudaEventDestroy(e);
@@ -613,6 +710,19 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
             return bail(fail(SALEC_ERR_ALLOC, "Laplacian mask"));
         if (cudaMemsetAsync(h->lap_mask, 0, words * sizeof(unsigned), h->stream) != cudaSuccess)
             return bail(fail(SALEC_ERR_CUDA, "Laplacian mask memset"));
+    }
+    {
+        std::vector<int> ident(d.R);
+        for (int j = 0; j < d.R; ++j) ident[j] = j;
+        if (cudaMalloc(&h->row_identity, sizeof(int) * d.R) != cudaSuccess)
+            return bail(fail(SALEC_ERR_ALLOC, "row map"));
+        if (cudaMemcpy(h->row_identity, ident.data(), sizeof(int) * d.R, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(fail(SALEC_ERR_CUDA, "row map upload"));
+        for (int k = 0; k < 5; ++k) {
+            h->geo[k].tab = field_ptr(h, field_by_name(kGeoFields[k]));
+            h->geo[k].row = h->row_identity;
+            h->geo[k].plane = d.PL;
+        }
     }
 
     std::vector<DevMat> dms(d.nmat);

@@ -17,6 +17,8 @@ namespace salec {
 
 #define KIDX(i, j) ((long long)(i) + (long long)c.d.P * (long long)(j))
 #define PLN(ptr, comp) ((ptr) + (long long)(comp) * c.d.PL)
+// component comp of a row-tabled geometry field at the thread's own point (i, j)
+#define GEO(g, comp) ((g).tab[(long long)(comp) * (g).plane + i + (long long)c.d.P * (g).row[j]])
 
 template <class C>
 __device__ __forceinline__ bool cell_interior(const C &c, int i, int j)
@@ -119,7 +121,7 @@ __device__ __forceinline__ void vertex_momentum(const C &c, int i, int j)
         if (PLN(c.f.e_wpt, corner[k])[cl[k]] > 0.) void_corner++;
         const double rho = c.f.e_den[cl[k]];
         if (rho < SALEC_TOLRHO) continue;
-        const double lv = PLN(c.f.v_vol, k + 1)[p];
+        const double lv = GEO(c.g_v_vol, k + 1);
         vvol += lv;
         vmass += rho * lv;
         const double w = rho * lv;
@@ -244,7 +246,7 @@ __global__ void k_gradient_viscosity_cfl(const CtxT<R> c)
         double vx[4], vy[4];
         for (int k = 0; k < 4; ++k) { vx[k] = c.f.v_vel[vl[k]]; vy[k] = PLN(c.f.v_vel, 1)[vl[k]]; }
         double g[12];
-        for (int k = 0; k < 12; ++k) g[k] = PLN(c.f.e_grad, k)[p];
+        for (int k = 0; k < 12; ++k) g[k] = GEO(c.g_e_grad, k);
         double d0 = 0., d1 = 0., d2 = 0., d3 = 0., d4 = 0.;
         for (int k = 0; k < 4; ++k) d0 += g[k] * vx[k];        // dv_r/dr
         for (int k = 0; k < 4; ++k) d2 += g[k] * vy[k];        // dv_z/dr
@@ -264,7 +266,7 @@ __global__ void k_gradient_viscosity_cfl(const CtxT<R> c)
         if (vof0 > SALEC_TOLVOF || c.f.e_pre[p] <= 0.0) {
             q = 0.;
         } else {
-            double area = c.f.e_vol[p] / c.f.e_pos[p];
+            double area = GEO(c.g_e_vol, 0) / c.f.e_pos[p];
             area = fabs(area);
             const double ql = c.rp.avis1 * csd * sqrt(area);
             const double qq = c.rp.avis2 * div * area;
@@ -522,7 +524,7 @@ __global__ void k_vertex_acceleration(const CtxT<R> c)
     const double dt = c.scal->dt;
     double ax = 0., ay = 0., vmass = 0., vvol = 0.;
     double sub[4];
-    for (int k = 0; k < 4; ++k) sub[k] = PLN(c.f.v_subvol, k)[p];
+    for (int k = 0; k < 4; ++k) sub[k] = GEO(c.g_v_subvol, k);
     double sigx = 0., sigy = 0.;
     double alx = 0., aly = 0.;
     if (pml) {
@@ -533,7 +535,7 @@ __global__ void k_vertex_acceleration(const CtxT<R> c)
     const bool damped = pml && (sigx > 0. || sigy > 0.);
     for (int k = 0; k < 4; ++k) {
         const long long e = cl[k];
-        const double sfx = PLN(c.f.v_suf, 2 * k)[p], sfy = PLN(c.f.v_suf, 2 * k + 1)[p];
+        const double sfx = GEO(c.g_v_suf, 2 * k), sfy = GEO(c.g_v_suf, 2 * k + 1);
         const double lp = c.f.e_pre[e] + c.f.e_q[e];
         const double ste0 = c.f.e_ste[e], ste1 = PLN(c.f.e_ste, 1)[e], ste2 = PLN(c.f.e_ste, 2)[e],
                      ste3 = PLN(c.f.e_ste, 3)[e];
@@ -566,7 +568,7 @@ __global__ void k_vertex_acceleration(const CtxT<R> c)
                 alx += (sigx + sigy) * sub[k] * sth * dt;
             }
         }
-        const double lv = PLN(c.f.v_vol, 1 + k)[p];
+        const double lv = GEO(c.g_v_vol, 1 + k);
         vmass += lv * c.f.e_den[e];
         vvol += lv;
     }
@@ -963,7 +965,7 @@ __global__ void __launch_bounds__(256) k_flux(const CtxT<R> c, int pass)
     } else {
         double grd[12];
         #pragma unroll
-        for (int k = 0; k < 8; ++k) grd[k] = PLN(c.f.e_grad, k)[p];
+        for (int k = 0; k < 8; ++k) grd[k] = GEO(c.g_e_grad, k);
         double gx = 0., gy = 0.;
         {
             const auto *vv = PLN(c.f.v_vof, prim);
