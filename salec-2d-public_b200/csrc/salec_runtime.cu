@@ -149,6 +149,11 @@ struct salec_gpu {
     // tracer arrays, so changing either drops the graph)
     cudaGraphExec_t cycle_graph = nullptr;
     long long cycle_graph_launches = 0;
+    // in the captured cycle the tracer sweep runs on a side stream beside the flux sweep (it
+    // reads nothing the flux writes and writes only tracer arrays); joined before phase 13
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool fork_tracers = false;
     void *output = nullptr;     // output writer state (salec_output.cu)
 
     template <class R>
@@ -298,13 +303,23 @@ int run_phase_t(salec_gpu *h, int ph)
         rc = run_gather(h, h->r_dis);
         break;
     case 10: launch_step_kernel(SK_ENERGY, c, s); break;
-    case 11: launch_step_kernel(SK_TRACERS, c, s); break;
+    case 11:
+        if (h->fork_tracers && h->tr.n > 0) {
+            CUDA_TRY(cudaEventRecord(h->ev_fork, s));
+            CUDA_TRY(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+            launch_step_kernel(SK_TRACERS, c, h->side);
+            CUDA_TRY(cudaEventRecord(h->ev_join, h->side));
+        } else {
+            launch_step_kernel(SK_TRACERS, c, s);
+        }
+        break;
     case 12:
         launch_step_kernel(SK_FLUX, c, s, 0);
         rc = run_gather(h, h->g_flux_state);
         launch_step_kernel(SK_FLUX, c, s, 1);
         break;
     case 13:   // strength condition: count the lubricating tracers of every cell in e_cnd
+        if (h->fork_tracers && h->tr.n > 0) CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));
         if (h->rp.tracer_lubrication > 0) {
             const int fid = field_by_name("e_cnd");
             CUDA_TRY(cudaMemsetAsync(field_ptr(h, fid), 0, (size_t)h->d.PL * field_elem(h, fid), s));
@@ -538,6 +553,9 @@ void release(salec_gpu *h)
     if (h->cycle_graph) cudaGraphExecDestroy(h->cycle_graph);
     for (auto e : h->ev_a) cudaEventDestroy(e);
     for (auto e : h->ev_b) cudaEventDestroy(e);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -684,6 +702,10 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
     rp.tracer_lub_frac = run->tracer_lub_frac; rp.max_dt = run->max_dt;
 
     auto bail = [&](int rc) { release(h); return rc; };
+    if (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess)
+        return bail(fail(SALEC_ERR_CUDA, "side stream or events"));
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(SALEC_ERR_CUDA, "cudaStreamCreate failed"));
 
@@ -830,7 +852,9 @@ void capture_cycle_graph(salec_gpu *h)
         return;
     }
     int rc = SALEC_OK;
+    h->fork_tracers = true;
     for (int p = 0; p <= 15 && rc == SALEC_OK; ++p) rc = run_phase(h, p);
+    h->fork_tracers = false;
     const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->launches = before;
     if (rc != SALEC_OK || e != cudaSuccess || !g) {
