@@ -113,3 +113,30 @@ def oracle_output_cases(kinds: List[str], nsteps: int, root: str) -> Dict[str, D
     with cf.ProcessPoolExecutor(max_workers=max(1, min(len(kinds), os.cpu_count() or 1)), mp_context=ctx) as ex:
         futs = {k: ex.submit(oracle_output_case, k, nsteps, os.path.join(root, k)) for k in kinds}
         return {k: f.result() for k, f in futs.items()}
+
+
+CONFIG1_FIELDS = ["e_den", "e_pre", "m_eng", "m_vof", "v_vel", "e_ste", "e_dam", "y_profile"]
+
+
+def oracle_config_run(deck_fn: str, checkpoints: List[int], folder: str) -> Dict:
+    """The reference's own initialisation and time loop on a named deck (decks.<deck_fn>()),
+    recording CONFIG1_FIELDS, dt and time at each checkpoint cycle."""
+    d = getattr(bridge.decks, deck_fn)()
+    deck = bridge.decks.write_deck(d, folder)
+    ref.init(deck, folder, os.path.join(folder, "run"))
+    out = {"deck": deck, "folder": folder, "at": {}}
+    done = 0
+    for k in checkpoints:
+        ref.step(k - done)
+        done = k
+        rec = {n: ref.get(n) for n in CONFIG1_FIELDS}
+        rec["dt"] = ref.scalar("dt")
+        rec["time"] = ref.scalar("time")
+        out["at"][k] = rec
+    return out
+
+
+def oracle_config_run_isolated(deck_fn: str, checkpoints: List[int], folder: str) -> Dict:
+    ctx = mp.get_context("spawn")
+    with cf.ProcessPoolExecutor(max_workers=1, mp_context=ctx) as ex:
+        return ex.submit(oracle_config_run, deck_fn, checkpoints, folder).result()
