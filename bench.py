@@ -319,6 +319,7 @@ def run_gpu_arm(args):
         init_state[name] = buf
     init_tracers = sim.get_tracers()
 
+    shapes = sim.autotune(cycles=4)   # untimed; block shapes of the 2-D sweeps for this mesh
     sim.step(args.warmup)
     sim.sync()
     stream = torch.cuda.ExternalStream(sim.stream())
@@ -420,6 +421,7 @@ def run_gpu_arm(args):
     mixed = None
     if not args.no_mixed:
         mix = capi.Simulation.from_deck(deck, tmp, precision=capi.PRECISION_MIXED)
+        mix.autotune(cycles=4)
         mix.step(args.warmup)
         mix.sync()
         mstream = torch.cuda.ExternalStream(mix.stream())
@@ -481,7 +483,8 @@ def run_gpu_arm(args):
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "state %.1f GB, each step moves >= %.1f GB > 126 MB L2 (no flush needed)"
                              % (h2d / 1e9, kernel_bytes_step / 1e9),
-                       "init_s": round(init_s, 2), "point_classes": counts, "tracers": ntr},
+                       "init_s": round(init_s, 2), "point_classes": counts, "tracers": ntr,
+                       "block_shapes": {PHASE_KERNELS[p]: list(v) for p, v in shapes.items()}},
             "roofline": {"bound": "hbm", "kernel": PHASE_KERNELS[dom], "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": profile_traffic(PHASE_KERNELS[dom], cells), "bytes_per_launch": dom_bytes,
@@ -534,6 +537,9 @@ def run_ensemble(args):
 
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         sims = list(ex.map(make, paths))
+    if args.ens_autotune:
+        for s in sims:
+            s.autotune(cycles=2)   # block shapes per member mesh, part of the timed initialisation
     torch.cuda.synchronize()
     init_s = ranks.all_max(time.perf_counter() - t0)
     cells = [s.run.nx * s.run.ny for s in sims]
@@ -587,6 +593,8 @@ def main():
     ap.add_argument("--ens-chunk", type=int, default=32)
     ap.add_argument("--ens-seed", type=int, default=2024)
     ap.add_argument("--ens-precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--ens-autotune", action="store_true",
+                    help="tune the block shapes of every member (costs more than it saves at 2000 cycles)")
     args = ap.parse_args()
     if args.warmup < 1:
         args.warmup = 1

@@ -161,6 +161,13 @@ int salec_gpu_step_many(salec_gpu *const *handles, int n, int nsteps, int chunk)
  * energy, 11 tracers, 12 face fluxes (+ ghosts), 13 strength condition, 14 remap, damping,
  * ejecta drag and EOS, 15 cycle control. */
 int salec_gpu_phases(salec_gpu *h, int first, int last);
+/* Pick the block shape of every 2-D sweep for this handle's mesh: each candidate shape is
+ * timed per phase over `cycles` cycles (after one warm-up cycle) from a device snapshot of the
+ * state, the fastest is kept per sweep, and the snapshot is restored, so the simulation is left
+ * exactly where it was. The shape changes no result (one thread per point, exact reductions).
+ * Takes a device copy of the field pool for its duration. If shapes is not NULL it receives 10
+ * triples (phase, block x, block y). No counterpart in the reference. */
+int salec_gpu_autotune(salec_gpu *h, int cycles, int *shapes);
 /* Block until the handle's stream is idle. */
 int salec_gpu_sync(salec_gpu *h);
 /* The CUDA stream (cudaStream_t) all work of the handle is queued on. */

@@ -49,14 +49,16 @@ enum StepKernel {
     SK_PROFILE_RESET, SK_TRACE_PROFILE, SK_PROFILE_DECODE, SK_VERTEX_VOF_MOMENTUM, SK_CELL_VELOCITY,
     SK_VOID_VERTICES, SK_GRADIENT, SK_FINALIZE_DT, SK_STRESS, SK_ACCELERATION, SK_DISPLACEMENT, SK_ENERGY,
     SK_TRACERS, SK_FLUX, SK_REMAP_DAMP_STATE, SK_CYCLE, SK_RECORD_REFERENCE, SK_INIT_VERTEX_VELOCITY,
-    SK_STRENGTH_CONDITION, SK_LAPLACE_MASK
+    SK_STRENGTH_CONDITION, SK_LAPLACE_MASK, SK_COUNT
 };
 
 #ifdef __CUDACC__
 // flux: a0 = pass (0 interior, 1 pad); remap: a0..a3 = remap, damping, ejecta drag, EOS switches
+// blk is the block shape of the 2-D sweeps (cells, faces, vertices); the surface profile, the
+// Laplacian mask, the tracer and the single-thread kernels use their own fixed shapes.
 template <class R>
-void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, int a0 = 0, int a1 = 0, int a2 = 0,
-                        int a3 = 0);
+void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, dim3 blk, int a0 = 0, int a1 = 0,
+                        int a2 = 0, int a3 = 0);
 __global__ void k_gather(GatherBatch g, int mode, double *scratch);
 void launch_aos_to_planes(const double *aos, void *base, bool f32, long long plane, int P, int nx, int ny, int nc,
                           cudaStream_t s);

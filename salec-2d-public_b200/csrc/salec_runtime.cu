@@ -128,6 +128,7 @@ struct salec_gpu {
     Gather g_mvof, g_dvel_den, g_evel, g_pre_ste_q, g_flux_state, r_vel, r_acc, r_dis, g_init;
     Tracers tr{};
     void *tr_block = nullptr;   // one allocation holding every tracer array
+    size_t tr_bytes = 0;
     unsigned *lap_mask = nullptr;   // vertices with a non-zero Laplacian weight (1 bit each)
     // geometry fields read through tables of their distinct rows: v_vol, v_subvol, v_suf,
     // e_grad, e_vol (tab and row are owned when compact)
@@ -145,6 +146,7 @@ struct salec_gpu {
     std::vector<int> ev_phase;
     size_t ev_used = 0;
     long long launches = 0;     // kernels launched by this handle
+    dim3 blk[SK_COUNT];         // block shape of each 2-D sweep (salec_gpu_autotune picks them)
     // one full cycle captured as a CUDA graph (kernel arguments hold the run parameters and the
     // tracer arrays, so changing either drops the graph)
     cudaGraphExec_t cycle_graph = nullptr;
@@ -274,65 +276,65 @@ int run_phase_t(salec_gpu *h, int ph)
     h->launches += kLaunches[ph] + (ph == 11 && h->tr.n > 0 ? 1 : 0);
     switch (ph) {
     case 0:
-        launch_step_kernel(SK_PROFILE_RESET, c, s);
-        launch_step_kernel(SK_TRACE_PROFILE, c, s);
-        launch_step_kernel(SK_PROFILE_DECODE, c, s);
+        launch_step_kernel(SK_PROFILE_RESET, c, s, h->blk[SK_PROFILE_RESET]);
+        launch_step_kernel(SK_TRACE_PROFILE, c, s, h->blk[SK_TRACE_PROFILE]);
+        launch_step_kernel(SK_PROFILE_DECODE, c, s, h->blk[SK_PROFILE_DECODE]);
         break;
     case 1:   // vertex volume fractions and vertex momentum in one sweep (phase 2 is empty)
         rc = run_gather(h, h->g_mvof);
         if (!rc) rc = run_gather(h, h->g_dvel_den);
-        launch_step_kernel(SK_VERTEX_VOF_MOMENTUM, c, s);
+        launch_step_kernel(SK_VERTEX_VOF_MOMENTUM, c, s, h->blk[SK_VERTEX_VOF_MOMENTUM]);
         if (!rc) rc = run_gather(h, h->r_vel);
         break;
     case 2: break;
     case 3:
-        launch_step_kernel(SK_CELL_VELOCITY, c, s);
+        launch_step_kernel(SK_CELL_VELOCITY, c, s, h->blk[SK_CELL_VELOCITY]);
         rc = run_gather(h, h->g_evel);
         break;
-    case 4: launch_step_kernel(SK_VOID_VERTICES, c, s); break;
-    case 5: launch_step_kernel(SK_GRADIENT, c, s); break;
-    case 6: launch_step_kernel(SK_FINALIZE_DT, c, s); break;
-    case 7: launch_step_kernel(SK_STRESS, c, s); break;
+    case 4: launch_step_kernel(SK_VOID_VERTICES, c, s, h->blk[SK_VOID_VERTICES]); break;
+    case 5: launch_step_kernel(SK_GRADIENT, c, s, h->blk[SK_GRADIENT]); break;
+    case 6: launch_step_kernel(SK_FINALIZE_DT, c, s, h->blk[SK_FINALIZE_DT]); break;
+    case 7: launch_step_kernel(SK_STRESS, c, s, h->blk[SK_STRESS]); break;
     case 8:
         rc = run_gather(h, h->g_pre_ste_q);
-        launch_step_kernel(SK_ACCELERATION, c, s);
+        launch_step_kernel(SK_ACCELERATION, c, s, h->blk[SK_ACCELERATION]);
         if (!rc) rc = run_gather(h, h->r_acc);
         break;
     case 9:
-        launch_step_kernel(SK_DISPLACEMENT, c, s);
+        launch_step_kernel(SK_DISPLACEMENT, c, s, h->blk[SK_DISPLACEMENT]);
         rc = run_gather(h, h->r_dis);
         break;
-    case 10: launch_step_kernel(SK_ENERGY, c, s); break;
+    case 10: launch_step_kernel(SK_ENERGY, c, s, h->blk[SK_ENERGY]); break;
     case 11:
         if (h->fork_tracers && h->tr.n > 0) {
             CUDA_TRY(cudaEventRecord(h->ev_fork, s));
             CUDA_TRY(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
-            launch_step_kernel(SK_TRACERS, c, h->side);
+            launch_step_kernel(SK_TRACERS, c, h->side, h->blk[SK_TRACERS]);
             CUDA_TRY(cudaEventRecord(h->ev_join, h->side));
         } else {
-            launch_step_kernel(SK_TRACERS, c, s);
+            launch_step_kernel(SK_TRACERS, c, s, h->blk[SK_TRACERS]);
         }
         break;
     case 12:
-        launch_step_kernel(SK_FLUX, c, s, 0);
+        launch_step_kernel(SK_FLUX, c, s, h->blk[SK_FLUX], 0);
         rc = run_gather(h, h->g_flux_state);
-        launch_step_kernel(SK_FLUX, c, s, 1);
+        launch_step_kernel(SK_FLUX, c, s, h->blk[SK_FLUX], 1);
         break;
     case 13:   // strength condition: count the lubricating tracers of every cell in e_cnd
         if (h->fork_tracers && h->tr.n > 0) CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));
         if (h->rp.tracer_lubrication > 0) {
             const int fid = field_by_name("e_cnd");
             CUDA_TRY(cudaMemsetAsync(field_ptr(h, fid), 0, (size_t)h->d.PL * field_elem(h, fid), s));
-            launch_step_kernel(SK_STRENGTH_CONDITION, c, s);
+            launch_step_kernel(SK_STRENGTH_CONDITION, c, s, h->blk[SK_STRENGTH_CONDITION]);
             if (h->tr.n > 0) h->launches += 1;
         }
         break;
     case 14: {
         const int ejecta = (h->rp.flow_resistance > 0. || h->rp.flow_friction > 0.) ? 1 : 0;
-        launch_step_kernel(SK_REMAP_DAMP_STATE, c, s, 1, 1, ejecta, 1);
+        launch_step_kernel(SK_REMAP_DAMP_STATE, c, s, h->blk[SK_REMAP_DAMP_STATE], 1, 1, ejecta, 1);
         break;
     }
-    case 15: launch_step_kernel(SK_CYCLE, c, s); break;
+    case 15: launch_step_kernel(SK_CYCLE, c, s, h->blk[SK_CYCLE]); break;
     default: return fail(SALEC_ERR_ARG, "phase out of range");
     }
     if (rc) return rc;
@@ -521,8 +523,8 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
                 if (rc) return rc;
             }
         if (!strcmp(kFields[fid].name, "v_laplace")) {
-            if (h->mixed) launch_step_kernel(SK_LAPLACE_MASK, h->ctx_t<float>(), h->stream);
-            else launch_step_kernel(SK_LAPLACE_MASK, h->ctx_t<double>(), h->stream);
+            if (h->mixed) launch_step_kernel(SK_LAPLACE_MASK, h->ctx_t<float>(), h->stream, h->blk[SK_LAPLACE_MASK]);
+            else launch_step_kernel(SK_LAPLACE_MASK, h->ctx_t<double>(), h->stream, h->blk[SK_LAPLACE_MASK]);
             CUDA_TRY(cudaGetLastError());
         }
         CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -564,11 +566,11 @@ template <class R>
 int finish_init_t(salec_gpu *h, double damp_time_in, double *damp_time_out)
 {
     const CtxT<R> c = h->ctx_t<R>();
-    launch_step_kernel(SK_REMAP_DAMP_STATE, c, h->stream, 0, 0, 0, 1);
+    launch_step_kernel(SK_REMAP_DAMP_STATE, c, h->stream, h->blk[SK_REMAP_DAMP_STATE], 0, 0, 0, 1);
     int rc = run_gather(h, h->g_init);
     if (rc) return rc;
     CUDA_TRY(cudaMemsetAsync(&h->scal->aux, 0, sizeof(unsigned long long), h->stream));
-    launch_step_kernel(SK_RECORD_REFERENCE, c, h->stream);
+    launch_step_kernel(SK_RECORD_REFERENCE, c, h->stream, h->blk[SK_RECORD_REFERENCE]);
     CUDA_TRY(cudaGetLastError());
     unsigned long long mx = 0;
     CUDA_TRY(cudaMemcpyAsync(&h->scal_host->aux, &h->scal->aux, sizeof(mx), cudaMemcpyDeviceToHost, h->stream));
@@ -578,7 +580,7 @@ int finish_init_t(salec_gpu *h, double damp_time_in, double *damp_time_out)
     const double dt2 = local * 2.0;
     h->rp.damp_time = dmax(dt2, damp_time_in);
     if (damp_time_out) *damp_time_out = h->rp.damp_time;
-    launch_step_kernel(SK_INIT_VERTEX_VELOCITY, h->ctx_t<R>(), h->stream);
+    launch_step_kernel(SK_INIT_VERTEX_VELOCITY, h->ctx_t<R>(), h->stream, h->blk[SK_INIT_VERTEX_VELOCITY]);
     CUDA_TRY(cudaGetLastError());
     for (const char *nm : {"e_vel", "e_ste", "e_dvel"}) {
         int fid = field_by_name(nm);
@@ -675,6 +677,7 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
     if (run->precision != SALEC_PRECISION_FP64 && run->precision != SALEC_PRECISION_MIXED)
         return fail(SALEC_ERR_ARG, "precision must be SALEC_PRECISION_FP64 or SALEC_PRECISION_MIXED");
     salec_gpu *h = new salec_gpu();
+    for (int k = 0; k < SK_COUNT; ++k) h->blk[k] = dim3(32, 4);
     Dims &d = h->d;
     d.nmat = run->nmat;
     d.enx = run->nx + 4;
@@ -947,6 +950,78 @@ int salec_gpu_phase_times(salec_gpu *h, double *ms, long long *count)
     return SALEC_OK;
 }
 
+int salec_gpu_autotune(salec_gpu *h, int cycles, int *shapes)
+{
+    if (!h || cycles < 1) return fail(SALEC_ERR_ARG, "bad argument");
+    static const dim3 cand[] = {dim3(32, 4), dim3(32, 8), dim3(64, 2), dim3(32, 2), dim3(64, 4), dim3(128, 1)};
+    constexpr int ncand = sizeof(cand) / sizeof(cand[0]);
+    // the 2-D sweeps of each phase
+    static const int tuned_phase[] = {1, 3, 4, 5, 7, 8, 9, 10, 12, 14};
+    static const StepKernel tuned_kernel[] = {SK_VERTEX_VOF_MOMENTUM, SK_CELL_VELOCITY, SK_VOID_VERTICES, SK_GRADIENT,
+                                              SK_STRESS, SK_ACCELERATION, SK_DISPLACEMENT, SK_ENERGY, SK_FLUX,
+                                              SK_REMAP_DAMP_STATE};
+    constexpr int ntuned = sizeof(tuned_phase) / sizeof(tuned_phase[0]);
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    // snapshot of everything the cycles change: the field pool, the scalars and the tracers
+    void *snap = nullptr, *snap_tr = nullptr;
+    Scal scal_host{};
+    CUDA_TRY(cudaMemcpy(&scal_host, h->scal, sizeof(Scal), cudaMemcpyDeviceToHost));
+    if (cudaMalloc(&snap, h->pool_bytes) != cudaSuccess) return fail(SALEC_ERR_ALLOC, "autotune snapshot");
+    if (h->tr_bytes && cudaMalloc(&snap_tr, h->tr_bytes) != cudaSuccess) {
+        cudaFree(snap);
+        return fail(SALEC_ERR_ALLOC, "autotune snapshot");
+    }
+    auto restore = [&]() -> int {
+        CUDA_TRY(cudaMemcpyAsync(h->pool, snap, h->pool_bytes, cudaMemcpyDeviceToDevice, h->stream));
+        if (snap_tr) CUDA_TRY(cudaMemcpyAsync(h->tr_block, snap_tr, h->tr_bytes, cudaMemcpyDeviceToDevice, h->stream));
+        CUDA_TRY(cudaMemcpyAsync(h->scal, &scal_host, sizeof(Scal), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        return SALEC_OK;
+    };
+    int rc = SALEC_OK;
+    if (cudaMemcpyAsync(snap, h->pool, h->pool_bytes, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess ||
+        (snap_tr && cudaMemcpyAsync(snap_tr, h->tr_block, h->tr_bytes, cudaMemcpyDeviceToDevice, h->stream) != cudaSuccess))
+        rc = fail(SALEC_ERR_CUDA, "autotune snapshot copy");
+    std::vector<double> best_ms(ntuned, 1e300);
+    std::vector<int> best(ntuned, 0);
+    const int was_profiling = h->profiling;
+    for (int ci = 0; ci < ncand && rc == SALEC_OK; ++ci) {
+        for (int t = 0; t < ntuned; ++t) h->blk[tuned_kernel[t]] = cand[ci];
+        if ((rc = restore())) break;
+        h->profiling = 1;
+        h->ev_used = 0;
+        for (int cy = 0; cy < cycles + 1 && rc == SALEC_OK; ++cy) {
+            if (cy == 1) h->ev_used = 0;   // the first cycle warms up
+            rc = salec_gpu_phases(h, 0, 15);
+        }
+        if (rc) break;
+        double ms[16];
+        long long cnt[16];
+        if ((rc = salec_gpu_phase_times(h, ms, cnt))) break;
+        for (int t = 0; t < ntuned; ++t) {
+            const int p = tuned_phase[t];
+            const double m = cnt[p] ? ms[p] / cnt[p] : 1e300;
+            if (m < best_ms[t]) { best_ms[t] = m; best[t] = ci; }
+        }
+    }
+    h->profiling = was_profiling;
+    h->ev_used = 0;
+    for (int t = 0; t < ntuned; ++t) h->blk[tuned_kernel[t]] = cand[best[t]];
+    const int rc2 = restore();
+    cudaFree(snap);
+    if (snap_tr) cudaFree(snap_tr);
+    if (h->cycle_graph) { cudaGraphExecDestroy(h->cycle_graph); h->cycle_graph = nullptr; }
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (shapes)
+        for (int t = 0; t < ntuned; ++t) {
+            shapes[3 * t] = tuned_phase[t];
+            shapes[3 * t + 1] = (int)cand[best[t]].x;
+            shapes[3 * t + 2] = (int)cand[best[t]].y;
+        }
+    return SALEC_OK;
+}
+
 int salec_gpu_sync(salec_gpu *h)
 {
     if (!h) return fail(SALEC_ERR_ARG, "null handle");
@@ -1002,6 +1077,7 @@ int salec_gpu_set_tracers(salec_gpu *h, int n, const double *rows)
     auto rounded = [](size_t sz) { return ((sz + 255) / 256) * 256; };
     const size_t bytes = nd * rounded((size_t)n * 8) + (nf + ni) * rounded((size_t)n * 4);
     CUDA_TRY(cudaMalloc(&h->tr_block, bytes));
+    h->tr_bytes = bytes;
     char *p = static_cast<char *>(h->tr_block);
     char *const end = p + bytes;
     auto take = [&](size_t sz) { char *q = p; p += rounded(sz); return q; };

@@ -1805,15 +1805,15 @@ void launch_count_nonfinite(const void *base, bool f32, long long n, unsigned lo
     } while (0)
 
 template <class R>
-void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, int a0, int a1, int a2, int a3)
+void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, dim3 b, int a0, int a1, int a2, int a3)
 {
-    const dim3 b(32, 8);
+    const dim3 b8(32, 8);
     const dim3 g((c.d.enx + b.x - 1) / b.x, (c.d.eny + b.y - 1) / b.y);   // cells (and faces)
     const dim3 gv((c.d.vnx + b.x - 1) / b.x, (c.d.vny + b.y - 1) / b.y);  // vertices
     const int ncol = (c.d.enx + 255) / 256;
     switch (k) {
     case SK_PROFILE_RESET: k_profile_reset<R><<<ncol, 256, 0, s>>>(c); break;
-    case SK_TRACE_PROFILE: k_trace_profile<R><<<dim3((c.d.enx + 31) / 32, (c.d.eny + 63) / 64), b, 0, s>>>(c); break;
+    case SK_TRACE_PROFILE: k_trace_profile<R><<<dim3((c.d.enx + 31) / 32, (c.d.eny + 63) / 64), b8, 0, s>>>(c); break;
     case SK_PROFILE_DECODE: k_profile_decode<R><<<ncol, 256, 0, s>>>(c); break;
     case SK_VERTEX_VOF_MOMENTUM: k_vertex_vof_momentum<R><<<gv, b, 0, s>>>(c); break;
     case SK_CELL_VELOCITY: k_cell_velocity<R><<<g, b, 0, s>>>(c); break;
@@ -1834,7 +1834,7 @@ void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, int a0, 
         else SALEC_NM_DISPATCH_P3(k_remap_damp_state, false, c, a0, a1, a2, a3);
         break;
     case SK_LAPLACE_MASK:
-        k_laplace_mask<R><<<dim3(c.d.P / 32, (c.d.vny + 7) / 8), b, 0, s>>>(c, const_cast<unsigned *>(c.lap_mask));
+        k_laplace_mask<R><<<dim3(c.d.P / 32, (c.d.vny + 7) / 8), b8, 0, s>>>(c, const_cast<unsigned *>(c.lap_mask));
         break;
     case SK_STRENGTH_CONDITION:
         if (c.tr.n > 0) k_strength_condition<R><<<(c.tr.n + 127) / 128, 128, 0, s>>>(c);
@@ -1845,7 +1845,7 @@ void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, int a0, 
     }
 }
 
-template void launch_step_kernel<double>(StepKernel, const CtxT<double> &, cudaStream_t, int, int, int, int);
-template void launch_step_kernel<float>(StepKernel, const CtxT<float> &, cudaStream_t, int, int, int, int);
+template void launch_step_kernel<double>(StepKernel, const CtxT<double> &, cudaStream_t, dim3, int, int, int, int);
+template void launch_step_kernel<float>(StepKernel, const CtxT<float> &, cudaStream_t, dim3, int, int, int, int);
 
 } // namespace salec

@@ -84,6 +84,7 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_get_field": ([vp, c_i, P_D, c_ll], c_i),
             "salec_gpu_step": ([vp, c_i], c_i),
             "salec_gpu_step_many": ([ctypes.POINTER(vp), c_i, c_i, c_i], c_i),
+            "salec_gpu_autotune": ([vp, c_i, ctypes.POINTER(c_i)], c_i),
             "salec_gpu_phases": ([vp, c_i, c_i], c_i),
             "salec_gpu_sync": ([vp], c_i),
             "salec_gpu_get_scalar": ([vp, ctypes.c_char_p, P_D], c_i),
@@ -303,6 +304,13 @@ class Simulation:
 
     def output_wait(self) -> None:
         _check(lib().salec_gpu_output_wait(self.h), "salec_gpu_output_wait")
+
+    def autotune(self, cycles: int = 4) -> dict:
+        """Pick the fastest block shape of every 2-D sweep for this mesh (state left unchanged);
+        returns {phase: (block x, block y)}."""
+        out = (c_i * 30)()
+        _check(lib().salec_gpu_autotune(self.h, int(cycles), out), "salec_gpu_autotune")
+        return {out[3 * k]: (out[3 * k + 1], out[3 * k + 2]) for k in range(10)}
 
     def check(self) -> int:
         n = c_ll()
