@@ -397,6 +397,10 @@ def run_gpu_arm(args):
     h2d = sum(a.nbytes for a in init_state.values()) + init_tracers.nbytes
     d2h_step = 8 * 2 + 8 * (n + 4)
     d2h_out = sum(8 * np.prod(sim.shape(f)) for f in out_fields)
+    out_bufs = {f: torch.empty(int(np.prod(sim.shape(f))), dtype=torch.float64, pin_memory=True).numpy()
+                .reshape(sim.shape(f)) for f in out_fields}
+    prof_buf = torch.empty(int(np.prod(sim.shape("y_profile"))), dtype=torch.float64,
+                           pin_memory=True).numpy().reshape(sim.shape("y_profile"))
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -404,14 +408,17 @@ def run_gpu_arm(args):
         sim.set_field(name, a)
     sim.set_tracers(init_tracers)
     sim.set_scalar("dt", run.dt)
+    t_up = time.perf_counter()
     for _ in range(args.steps):
         sim.step(1)
         sim.scalar("dt")
         sim.scalar("time")
-        sim.get_field("y_profile")
-    outs = [sim.get_field(f) for f in out_fields]
+        sim.get_field("y_profile", out=prof_buf)
+    t_loop = time.perf_counter()
+    outs = [sim.get_field(f, out=out_bufs[f]) for f in out_fields]
     sim.sync()
     e2e_s = time.perf_counter() - t0
+    e2e_parts = {"upload_s": t_up - t0, "cycles_s": t_loop - t_up, "download_s": e2e_s - (t_loop - t0)}
     e2e_s = all_max(e2e_s)
     e2e = world * cells * args.steps / e2e_s
     nbad = sim.check()
@@ -497,7 +504,7 @@ def run_gpu_arm(args):
                               "kernel_frac": kernel_bytes_step / (step_ms / 1000.0) / 1e9 / hbm},
             "kernels": per_kernel,
             "kernel_ms": breakdown,
-            "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": int(h2d / args.steps),
+            "e2e": {"value": e2e, "unit": "cell-updates/s", "parts": e2e_parts, "h2d_bytes_per_step": int(h2d / args.steps),
                     "d2h_bytes_per_step": int(d2h_step + d2h_out / args.steps)},
             "gpu_launches": launches,
             "clocks": clocks,

@@ -425,73 +425,163 @@ int upload_material(salec_gpu *h, const salec_material_desc &m, DevMat &dm)
 const char *const kGeoFields[5] = {"v_vol", "v_subvol", "v_suf", "e_grad", "e_vol"};
 constexpr int kGeoMaxRows = 512;   // more distinct rows than this: read the field's own planes
 
-// Table of the distinct rows of an uploaded geometry field (host AoS data `host`, nx x ny
-// points of nc components), compared bit for bit; mesh rows that repeat share one table row.
-int build_geo_table(salec_gpu *h, int slot, int fid, const double *host, int nx, int ny, int nc)
+// Row hashing for the geometry tables. Each row of an AoS field (row_doubles words) is
+// reduced to two 64-bit sums of a position-keyed splitmix64 finaliser of its words; the sums
+// commute, so a block reduces a row in any order and the result is deterministic. Rows that
+// hash alike are then compared word for word, so a collision costs a fallback, never a wrong
+// table.
+__device__ __forceinline__ unsigned long long geo_mix(unsigned long long z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+__global__ void __launch_bounds__(256) k_geo_row_hash(const unsigned long long *__restrict__ src, long long row_words,
+                                                      unsigned long long *__restrict__ out)
+{
+    const unsigned long long *r = src + (long long)blockIdx.x * row_words;
+    unsigned long long a = 0, b = 0;
+    for (long long k = threadIdx.x; k < row_words; k += blockDim.x) {
+        const unsigned long long w = r[k];
+        a += geo_mix(w + 0x9E3779B97F4A7C15ULL * (unsigned long long)(k + 1));
+        b += geo_mix((w ^ 0xD6E8FEB86659FD93ULL) + 0xC2B2AE3D27D4EB4FULL * (unsigned long long)(k + 7));
+    }
+    for (int o = 16; o; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    __shared__ unsigned long long sa[8], sb[8];
+    if ((threadIdx.x & 31) == 0) { sa[threadIdx.x >> 5] = a; sb[threadIdx.x >> 5] = b; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { a += sa[w]; b += sb[w]; }
+        out[2 * blockIdx.x] = a;
+        out[2 * blockIdx.x + 1] = b;
+    }
+}
+
+// Row j against its representative row rep[j]: any differing word sets *diff.
+__global__ void __launch_bounds__(256) k_geo_row_verify(const unsigned long long *__restrict__ src, long long row_words,
+                                                        const int *__restrict__ rep, unsigned *__restrict__ diff)
+{
+    const int j = blockIdx.x, q = rep[j];
+    if (q == j) return;
+    const unsigned long long *r = src + (long long)j * row_words, *t = src + (long long)q * row_words;
+    bool bad = false;
+    for (long long k = threadIdx.x; k < row_words; k += blockDim.x) bad |= r[k] != t[k];
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(diff, 1u);
+}
+
+// Distinct rows uniq[u] of src gathered into consecutive rows of dst.
+__global__ void __launch_bounds__(256) k_geo_row_gather(const unsigned long long *__restrict__ src, long long row_words,
+                                                        const int *__restrict__ uniq, unsigned long long *__restrict__ dst)
+{
+    const unsigned long long *r = src + (long long)uniq[blockIdx.x] * row_words;
+    unsigned long long *d = dst + (long long)blockIdx.x * row_words;
+    for (long long k = threadIdx.x; k < row_words; k += blockDim.x) d[k] = r[k];
+}
+
+// Table of the distinct rows of an uploaded geometry field, built from the AoS copy of the
+// field in the staging buffer (nx x ny points of nc components); mesh rows that repeat bit for
+// bit share one table row. The staging buffer is read in stream order after the upload.
+int build_geo_table(salec_gpu *h, int slot, int fid, int nx, int ny, int nc)
 {
     auto &g = h->geo[slot];
-    const size_t row_doubles = (size_t)nx * nc;
-    // row hashes on host threads, then the rows grouped in order (equal rows compared in full)
-    std::vector<unsigned long long> hashes(ny);
-    {
-        const int nt = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 16));
-        std::vector<std::thread> pool;
-        for (int t = 0; t < nt; ++t)
-            pool.emplace_back([&, t]() {
-                for (int j = t; j < ny; j += nt) {
-                    const double *r = host + (size_t)j * row_doubles;
-                    unsigned long long hsh = 1469598103934665603ULL;
-                    for (size_t k = 0; k < row_doubles; ++k) {
-                        unsigned long long w;
-                        memcpy(&w, r + k, sizeof(w));
-                        hsh = (hsh ^ w) * 0x9E3779B97F4A7C15ULL;
-                        hsh ^= hsh >> 29;
-                    }
-                    hashes[j] = hsh;
-                }
-            });
-        for (auto &th : pool) th.join();
-    }
-    std::unordered_map<unsigned long long, std::vector<int>> buckets;
-    std::vector<int> rowmap(h->d.R, 0), uniq;
-    for (int j = 0; j < ny; ++j) {
-        const double *r = host + (size_t)j * row_doubles;
-        const unsigned long long hsh = hashes[j];
-        int found = -1;
-        for (int u : buckets[hsh])
-            if (!memcmp(host + (size_t)uniq[u] * row_doubles, r, row_doubles * sizeof(double))) { found = u; break; }
-        if (found < 0) {
-            found = (int)uniq.size();
-            uniq.push_back(j);
-            buckets[hsh].push_back(found);
-        }
-        rowmap[j] = found;
-    }
+    const long long row_words = (long long)nx * nc;
     if (g.compact) { cudaFree(g.tab); cudaFree(g.row); }
     g = salec_gpu::GeoSlot();
     if (h->cycle_graph) { cudaGraphExecDestroy(h->cycle_graph); h->cycle_graph = nullptr; }
+    const auto *src = reinterpret_cast<const unsigned long long *>(h->staging);
+
+    unsigned long long *d_hash = nullptr;
+    CUDA_TRY(cudaMalloc(&d_hash, sizeof(unsigned long long) * 2 * ny));
+    k_geo_row_hash<<<ny, 256, 0, h->stream>>>(src, row_words, d_hash);
+    cudaError_t e = cudaGetLastError();
+    std::vector<unsigned long long> hashes(2 * (size_t)ny);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hashes.data(), d_hash, sizeof(unsigned long long) * 2 * ny, cudaMemcpyDeviceToHost,
+                            h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(d_hash);
+    CUDA_TRY(e);
+
+    // rows grouped in order of first appearance by their 128-bit hash
+    struct Key {
+        unsigned long long a, b;
+        bool operator==(const Key &o) const { return a == o.a && b == o.b; }
+    };
+    struct KeyHash {
+        size_t operator()(const Key &k) const { return (size_t)(k.a ^ (k.b * 0x9E3779B97F4A7C15ULL)); }
+    };
+    std::unordered_map<Key, int, KeyHash> first;
+    std::vector<int> rowmap(h->d.R, 0), rep(ny), uniq;
+    for (int j = 0; j < ny; ++j) {
+        const Key k{hashes[2 * (size_t)j], hashes[2 * (size_t)j + 1]};
+        auto it = first.find(k);
+        int u;
+        if (it == first.end()) {
+            u = (int)uniq.size();
+            uniq.push_back(j);
+            first.emplace(k, u);
+        } else {
+            u = it->second;
+        }
+        rowmap[j] = u;
+        rep[j] = uniq[u];
+    }
     const int U = (int)uniq.size();
-    if (U > kGeoMaxRows || U >= ny) {
+    auto full_planes = [&]() {
+        g = salec_gpu::GeoSlot();
         g.tab = field_ptr(h, fid);
         g.row = h->row_identity;
         g.plane = h->d.PL;
+    };
+    if (U > kGeoMaxRows || U >= ny) {
+        full_planes();
         return SALEC_OK;
     }
+
     const bool f32 = field_f32(h, fid);
     const long long plane = (((long long)U * h->d.P + 31) / 32) * 32;
-    std::vector<double> compact((size_t)U * row_doubles);
-    for (int u = 0; u < U; ++u)
-        memcpy(&compact[(size_t)u * row_doubles], host + (size_t)uniq[u] * row_doubles, row_doubles * sizeof(double));
-    CUDA_TRY(cudaMalloc(&g.tab, (size_t)nc * plane * field_elem(h, fid)));
-    CUDA_TRY(cudaMalloc(&g.row, sizeof(int) * h->d.R));
+    int *d_idx = nullptr;                   // rep[ny] then uniq[U]
+    unsigned *d_diff = nullptr;
+    unsigned long long *d_rows = nullptr;   // the U distinct rows, AoS
+    auto release_tmp = [&]() {
+        if (d_idx) cudaFree(d_idx);
+        if (d_diff) cudaFree(d_diff);
+        if (d_rows) cudaFree(d_rows);
+    };
+    e = cudaMalloc(&d_idx, sizeof(int) * ((size_t)ny + U));
+    if (e == cudaSuccess) e = cudaMalloc(&d_diff, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&d_rows, sizeof(unsigned long long) * (size_t)U * row_words);
+    if (e == cudaSuccess) e = cudaMalloc(&g.tab, (size_t)nc * plane * field_elem(h, fid));
+    if (e == cudaSuccess) e = cudaMalloc(&g.row, sizeof(int) * h->d.R);
     g.compact = true;
     g.plane = plane;
-    CUDA_TRY(cudaMemcpyAsync(h->staging, compact.data(), compact.size() * sizeof(double), cudaMemcpyHostToDevice,
-                             h->stream));
-    launch_aos_to_planes(h->staging, g.tab, f32, plane, h->d.P, nx, U, nc, h->stream);
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaMemcpyAsync(g.row, rowmap.data(), sizeof(int) * h->d.R, cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    unsigned diff = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_idx, rep.data(), sizeof(int) * ny, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_idx + ny, uniq.data(), sizeof(int) * U, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_diff, 0, sizeof(unsigned), h->stream);
+    if (e == cudaSuccess) {
+        k_geo_row_verify<<<ny, 256, 0, h->stream>>>(src, row_words, d_idx, d_diff);
+        k_geo_row_gather<<<U, 256, 0, h->stream>>>(src, row_words, d_idx + ny, d_rows);
+        launch_aos_to_planes(reinterpret_cast<const double *>(d_rows), g.tab, f32, plane, h->d.P, nx, U, nc,
+                             h->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(g.row, rowmap.data(), sizeof(int) * h->d.R, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&diff, d_diff, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    release_tmp();
+    if (e != cudaSuccess || diff) {
+        cudaFree(g.tab);
+        cudaFree(g.row);
+        full_planes();
+    }
+    CUDA_TRY(e);
     return SALEC_OK;
 }
 
@@ -519,7 +609,7 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
         CUDA_TRY(cudaGetLastError());
         for (int k = 0; k < 5; ++k)
             if (!strcmp(kFields[fid].name, kGeoFields[k])) {
-                int rc = build_geo_table(h, k, fid, host, nx, ny, nc);
+                int rc = build_geo_table(h, k, fid, nx, ny, nc);
                 if (rc) return rc;
             }
         if (!strcmp(kFields[fid].name, "v_laplace")) {
@@ -953,7 +1043,8 @@ int salec_gpu_phase_times(salec_gpu *h, double *ms, long long *count)
 int salec_gpu_autotune(salec_gpu *h, int cycles, int *shapes)
 {
     if (!h || cycles < 1) return fail(SALEC_ERR_ARG, "bad argument");
-    static const dim3 cand[] = {dim3(32, 4), dim3(32, 8), dim3(64, 2), dim3(32, 2), dim3(64, 4), dim3(128, 1)};
+    static const dim3 cand[] = {dim3(32, 4), dim3(32, 8), dim3(64, 2), dim3(32, 2), dim3(64, 4), dim3(128, 1),
+                                dim3(32, 1), dim3(64, 1)};
     constexpr int ncand = sizeof(cand) / sizeof(cand[0]);
     // the 2-D sweeps of each phase
     static const int tuned_phase[] = {1, 3, 4, 5, 7, 8, 9, 10, 12, 14};

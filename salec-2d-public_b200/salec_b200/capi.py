@@ -271,8 +271,14 @@ class Simulation:
         b = np.ascontiguousarray(a, dtype=np.float64).reshape(shp)
         _check(lib().salec_gpu_set_field(self.h, field_index(name), _ptr(b), b.size), "set_field " + name)
 
-    def get_field(self, name: str) -> np.ndarray:
-        out = np.empty(self.shape(name), dtype=np.float64)
+    def get_field(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """Download a field; `out`, when given, must be a C-contiguous float64 array of the
+        field's shape (pinned host memory makes the copy a direct DMA)."""
+        shp = self.shape(name)
+        if out is None:
+            out = np.empty(shp, dtype=np.float64)
+        elif out.dtype != np.float64 or tuple(out.shape) != tuple(shp) or not out.flags.c_contiguous:
+            raise ValueError(f"get_field {name}: out must be C-contiguous float64 of shape {shp}")
         _check(lib().salec_gpu_get_field(self.h, field_index(name), _ptr(out), out.size), "get_field " + name)
         return out
 
