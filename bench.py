@@ -333,7 +333,9 @@ def run_gpu_arm(args):
     sampler.start()
     launches0 = sim.scalar("launches")
     e0.record(stream)
+    torch.cuda.nvtx.range_push("timed_cycles")   # lets a profiler select exactly these launches
     sim.step(args.steps)
+    torch.cuda.nvtx.range_pop()
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1)

@@ -20,6 +20,70 @@ namespace salec {
 // component comp of a row-tabled geometry field at the thread's own point (i, j)
 #define GEO(g, comp) ((g).tab[(long long)(comp) * (g).plane + i + (long long)c.d.P * (g).row[j]])
 
+// Register budget per thread of the heavy sweeps: SALEC_REGS_<K> > 0 caps the allocator at that
+// many registers (__maxnreg__), trading a few spilled values that stay in L1 for more resident
+// warps to hide the dependent loads; 0 leaves the allocator's own choice under the default
+// bounds (256-thread blocks where a kernel declares them, else the 1024-thread default). The
+// defaults are the fastest budgets measured on B200 for the 2048x2048 impact in FP64 (registers
+// are granted per warp in units of 256, so only multiples of 8 differ); the budgets change
+// which values live in registers, never the arithmetic.
+#ifndef SALEC_REGS_STRESS
+#define SALEC_REGS_STRESS 56
+#endif
+#ifndef SALEC_REGS_FLUX
+#define SALEC_REGS_FLUX 80
+#endif
+#ifndef SALEC_REGS_REMAP
+#define SALEC_REGS_REMAP 96
+#endif
+#ifndef SALEC_REGS_ACCEL
+#define SALEC_REGS_ACCEL 40
+#endif
+#ifndef SALEC_REGS_VOFMOM
+#define SALEC_REGS_VOFMOM 32
+#endif
+#ifndef SALEC_REGS_GRAD
+#define SALEC_REGS_GRAD 40
+#endif
+#ifndef SALEC_REGS_ENERGY
+#define SALEC_REGS_ENERGY 40
+#endif
+#if SALEC_REGS_STRESS > 0
+#define SALEC_BOUNDS_STRESS __maxnreg__(SALEC_REGS_STRESS)
+#else
+#define SALEC_BOUNDS_STRESS __launch_bounds__(256)
+#endif
+#if SALEC_REGS_FLUX > 0
+#define SALEC_BOUNDS_FLUX __maxnreg__(SALEC_REGS_FLUX)
+#else
+#define SALEC_BOUNDS_FLUX __launch_bounds__(256)
+#endif
+#if SALEC_REGS_REMAP > 0
+#define SALEC_BOUNDS_REMAP __maxnreg__(SALEC_REGS_REMAP)
+#else
+#define SALEC_BOUNDS_REMAP __launch_bounds__(256)
+#endif
+#if SALEC_REGS_ENERGY > 0
+#define SALEC_BOUNDS_ENERGY __maxnreg__(SALEC_REGS_ENERGY)
+#else
+#define SALEC_BOUNDS_ENERGY __launch_bounds__(256)
+#endif
+#if SALEC_REGS_ACCEL > 0
+#define SALEC_BOUNDS_ACCEL __maxnreg__(SALEC_REGS_ACCEL)
+#else
+#define SALEC_BOUNDS_ACCEL
+#endif
+#if SALEC_REGS_VOFMOM > 0
+#define SALEC_BOUNDS_VOFMOM __maxnreg__(SALEC_REGS_VOFMOM)
+#else
+#define SALEC_BOUNDS_VOFMOM
+#endif
+#if SALEC_REGS_GRAD > 0
+#define SALEC_BOUNDS_GRAD __maxnreg__(SALEC_REGS_GRAD)
+#else
+#define SALEC_BOUNDS_GRAD
+#endif
+
 template <class C>
 __device__ __forceinline__ bool cell_interior(const C &c, int i, int j)
 {
@@ -154,7 +218,7 @@ __device__ __forceinline__ void vertex_momentum(const C &c, int i, int j)
 // Phases 1 and 2 in one vertex sweep: both read only cell fields that no vertex sweep writes,
 // so one thread per vertex does both (the m_vof and e_dvel/e_den ghost fills run first).
 template <class R>
-__global__ void k_vertex_vof_momentum(const CtxT<R> c)
+__global__ void SALEC_BOUNDS_VOFMOM k_vertex_vof_momentum(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!vert_active(c, i, j)) return;
@@ -236,7 +300,7 @@ __global__ void k_void_vertices(const CtxT<R> c)
 // artificial viscosity and the CFL candidate of every interior cell.
 // update_e_gradvel (src/sale2d.c:1144-1236) and calculate_dt (src/sale2d.c:1959-2016).
 template <class R>
-__global__ void k_gradient_viscosity_cfl(const CtxT<R> c)
+__global__ void SALEC_BOUNDS_GRAD k_gradient_viscosity_cfl(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     unsigned long long cand = ~0ULL;
@@ -307,7 +371,7 @@ __global__ void k_finalize_dt(const CtxT<R> c)
 // ============================================================ phase 7: vibration, stress, damage
 // block_vibration (src/strength.c:625-695) and update_e_stress (src/strength.c:7-349).
 template <class R, int NM, bool POR>
-__global__ void __launch_bounds__(256) k_stress(const CtxT<R> c)
+__global__ void SALEC_BOUNDS_STRESS k_stress(const CtxT<R> c)
 {
     constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -514,7 +578,7 @@ __global__ void __launch_bounds__(256) k_stress(const CtxT<R> c)
 // pressure + viscosity and deviatoric stress, hoop term, gravity and the nine-point
 // Laplacian damping (ANC); the PML form also integrates the auxiliary v_alpha.
 template <class R>
-__global__ void k_vertex_acceleration(const CtxT<R> c)
+__global__ void SALEC_BOUNDS_ACCEL k_vertex_acceleration(const CtxT<R> c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!vert_active(c, i, j)) return;
@@ -635,7 +699,7 @@ __global__ void k_vertex_displacement(const CtxT<R> c)
 // update_energy (src/sale2d.c:564-712) with the Wunnemann porosity update. After the vacuum
 // test, every input of the cell is loaded in one batch (no load waits on another).
 template <class R, int NM, bool POR>
-__global__ void __launch_bounds__(256) k_energy(const CtxT<R> c)
+__global__ void SALEC_BOUNDS_ENERGY k_energy(const CtxT<R> c)
 {
     constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -912,7 +976,7 @@ __device__ __forceinline__ void store_face(const CtxT<R> &c, double *f, double v
 
 // pass 0: interior cells; pass 1: pad cells (after the ghost fills of m_den, m_eng, ...).
 template <class R, int NM, bool POR>
-__global__ void __launch_bounds__(256) k_flux(const CtxT<R> c, int pass)
+__global__ void SALEC_BOUNDS_FLUX k_flux(const CtxT<R> c, int pass)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= c.d.enx || j >= c.d.eny) return;
@@ -1562,7 +1626,7 @@ __device__ __forceinline__ void state_cell(const CtxT<R> &c, long long p, const 
 // One thread per cell: remap (interior), damping (every cell, while t < damp_time), ejecta
 // drag and EOS (interior). The cell's state is stored once, after damping and drag.
 template <class R, int NM, bool POR, bool P3>
-__global__ void __launch_bounds__(256) k_remap_damp_state(const CtxT<R> c, int do_remap, int do_damp, int do_ejecta, int do_state)
+__global__ void SALEC_BOUNDS_REMAP k_remap_damp_state(const CtxT<R> c, int do_remap, int do_damp, int do_ejecta, int do_state)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= c.d.enx || j >= c.d.eny) return;
