@@ -35,7 +35,8 @@ sys.path.insert(0, ROOT)
 from salec_b200 import capi, decks, fields  # noqa: E402
 
 METRIC = "cell-updates/s"
-WORKLOAD = "impact 2048x2048 cells, SieDen granite + Tillotson ice, CPPR 40, 15 km/s, PML 30, FP64"
+def workload(n: int) -> str:
+    return "impact %dx%d cells, SieDen granite + Tillotson ice, CPPR 40, 15 km/s, PML 30, FP64" % (n, n)
 
 # ---------------------------------------------------------------- algorithmic bytes model
 # Bytes that each step kernel must move: every field its sweep reads, once, and every field
@@ -248,7 +249,7 @@ def run_reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "cell-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample": "%dx%d cells of the same deck" % (n, n),
+            "config": {"workload": workload(args.n), "sample": "%dx%d cells of the same deck" % (n, n),
                        "parallelism": "single host thread (the reference is single-threaded per rank)"},
             "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
                              "sample": "%d steps of a %dx%d-cell copy of the workload" % (args.steps, n, n)},
@@ -488,7 +489,7 @@ def run_gpu_arm(args):
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cells": cells, "materials": nmat, "form": "plain FP64",
+            "config": {"workload": workload(n), "cells": cells, "materials": nmat, "form": "plain FP64",
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "state %.1f GB, each step moves >= %.1f GB > 126 MB L2 (no flush needed)"
                              % (h2d / 1e9, kernel_bytes_step / 1e9),
