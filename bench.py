@@ -320,7 +320,11 @@ def run_gpu_arm(args):
         init_state[name] = buf
     init_tracers = sim.get_tracers()
 
-    shapes = sim.autotune(cycles=4)   # untimed; block shapes of the 2-D sweeps for this mesh
+    if args.block_shapes:   # shapes given (e.g. those a plain run tuned, for a profiler capture)
+        shapes = {int(p): tuple(v) for p, v in json.loads(args.block_shapes).items()}
+        sim.set_block_shapes(shapes)
+    else:
+        shapes = sim.autotune(cycles=4)   # untimed; block shapes of the 2-D sweeps for this mesh
     sim.step(args.warmup)
     sim.sync()
     stream = torch.cuda.ExternalStream(sim.stream())
@@ -494,7 +498,9 @@ def run_gpu_arm(args):
                        "l2": "state %.1f GB, each step moves >= %.1f GB > 126 MB L2 (no flush needed)"
                              % (h2d / 1e9, kernel_bytes_step / 1e9),
                        "init_s": round(init_s, 2), "point_classes": counts, "tracers": ntr,
-                       "block_shapes": {PHASE_KERNELS[p]: list(v) for p, v in shapes.items()}},
+                       "block_shapes": {PHASE_KERNELS[p]: list(v) for p, v in shapes.items()},
+                       "block_shapes_by_phase": {str(p): list(v) for p, v in shapes.items()},
+                       "block_shapes_source": "given" if args.block_shapes else "autotuned"},
             "roofline": {"bound": "hbm", "kernel": PHASE_KERNELS[dom], "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": profile_traffic(PHASE_KERNELS[dom], cells), "bytes_per_launch": dom_bytes,
@@ -548,8 +554,13 @@ def run_ensemble(args):
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         sims = list(ex.map(make, paths))
     if args.ens_autotune:
+        # block shapes tuned once, on the largest member, and shared: part of the timed
+        # initialisation
+        big = max(sims, key=lambda s: s.run.nx * s.run.ny)
+        tuned = big.autotune(cycles=2)
         for s in sims:
-            s.autotune(cycles=2)   # block shapes per member mesh, part of the timed initialisation
+            if s is not big:
+                s.set_block_shapes(tuned)
     torch.cuda.synchronize()
     init_s = ranks.all_max(time.perf_counter() - t0)
     cells = [s.run.nx * s.run.ny for s in sims]
@@ -604,7 +615,10 @@ def main():
     ap.add_argument("--ens-seed", type=int, default=2024)
     ap.add_argument("--ens-precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--ens-autotune", action="store_true",
-                    help="tune the block shapes of every member (costs more than it saves at 2000 cycles)")
+                    help="tune the block shapes on the largest member and set them on every member")
+    ap.add_argument("--block-shapes", default="",
+                    help='JSON {phase: [x, y]} of block shapes to set instead of autotuning, '
+                         'e.g. the "block_shapes_by_phase" of an earlier run')
     args = ap.parse_args()
     if args.warmup < 1:
         args.warmup = 1

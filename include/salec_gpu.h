@@ -168,6 +168,11 @@ int salec_gpu_phases(salec_gpu *h, int first, int last);
  * Takes a device copy of the field pool for its duration. If shapes is not NULL it receives 10
  * triples (phase, block x, block y). No counterpart in the reference. */
 int salec_gpu_autotune(salec_gpu *h, int cycles, int *shapes);
+/* Set the block shapes of the tunable 2-D sweeps from n triples (phase, block x, block y), as
+ * salec_gpu_autotune returns them, e.g. to reuse one member's tuning for others of the same
+ * mesh. Block x must be a multiple of 32 and x*y at most 256; any invalid triple rejects the
+ * whole call (SALEC_ERR_ARG) with no shape changed. No counterpart in the reference. */
+int salec_gpu_set_block_shapes(salec_gpu *h, const int *shapes, int n);
 /* Block until the handle's stream is idle. */
 int salec_gpu_sync(salec_gpu *h);
 /* The CUDA stream (cudaStream_t) all work of the handle is queued on. */

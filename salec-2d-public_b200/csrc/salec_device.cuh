@@ -52,6 +52,10 @@ struct DevMat {
     const double *cold_yeng;   // cold energy on the uniform density grid k*StepDen
     const double *xtem, *yden; // tabulated axes
     const double *data;        // [ntem][nden][3]
+    // bucket guesses of the axis searches (axis_search); null where an axis is not monotone
+    const int *xtem_bkt, *yden_bkt;
+    double xtem_b0, xtem_binv, yden_b0, yden_binv;
+    int xtem_nb, yden_nb;
 };
 
 // Run parameters fixed for the whole run (sale2d_var / mesh2d_info members).
@@ -191,6 +195,26 @@ __device__ __forceinline__ int bisearch(double x, const double *xs, int n)
     return lo;
 }
 
+// bisearch over a non-decreasing axis, started from a bucket guess. For x in [xs[0], xs[n-1])
+// the bisection ends at the unique k with xs[k] <= x < xs[k+1] (its loop keeps xs[lo] <= x <
+// xs[hi]); the guess bkt[(x - b0) * binv] is moved by the same comparisons until it satisfies
+// both, so the index is the bisection's whatever the rounding of the bucket number. Below,
+// above and NaN take the bisection's own exits (0, n-2, n-2). Typically two dependent loads
+// instead of log2(n).
+__device__ __forceinline__ int axis_search(double x, const double *xs, int n, const int *bkt, int nb, double b0,
+                                           double binv)
+{
+    if (!bkt) return bisearch(x, xs, n);
+    if (x < xs[0]) return 0;
+    if (!(x < xs[n - 1])) return n - 2;
+    int b = (int)((x - b0) * binv);
+    b = b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+    int g = bkt[b];
+    while (g < n - 2 && xs[g + 1] <= x) ++g;
+    while (g > 0 && xs[g] > x) --g;
+    return g;
+}
+
 // ------------------------------------------------------------------ Tillotson EOS
 // Tillotson (1962) as evaluated in src/eos/eos_state.c:322-438 (TillCold, TillHot, TillTran,
 // TillPres); t = {rho0, Cv, A, B, E0, a, b, alpha, beta, Eiv, Ecv, Tref, StepDen}.
@@ -260,8 +284,8 @@ __device__ __forceinline__ void sieden_state(const DevMat &m, double den, double
 {
     const double tden = den;
     const double teng = eng / den;
-    const int di = bisearch(tden, m.yden, m.nden), dj = di + 1;
-    const int ti = bisearch(teng, m.xtem, m.ntem), tj = ti + 1;
+    const int di = axis_search(tden, m.yden, m.nden, m.yden_bkt, m.yden_nb, m.yden_b0, m.yden_binv), dj = di + 1;
+    const int ti = axis_search(teng, m.xtem, m.ntem, m.xtem_bkt, m.xtem_nb, m.xtem_b0, m.xtem_binv), tj = ti + 1;
     const double dxr = (tden - m.yden[di]) / (m.yden[dj] - m.yden[di]);
     const double dxl = wind(1.0 - dxr, 0.0, 1.0);
     const double exr = (teng - m.xtem[ti]) / (m.xtem[tj] - m.xtem[ti]);
@@ -278,10 +302,17 @@ __device__ __forceinline__ void sieden_state(const DevMat &m, double den, double
 // Temperature-density table with energy rows searched per density: src/eos/eos_state.c:793-841.
 __device__ __forceinline__ void aneos_td_state(const DevMat &m, double den, double eng, double &tem, double &pre, double &csd)
 {
+    // on a monotone axis the bracketing loop of eos_state.c ends where axis_search does: 0 below
+    // the axis, n-2 above it and for NaN, else the k with yden[k] <= den < yden[k+1]
     int di = 0, dj = m.nden - 1;
-    while (di + 1 < dj) {
-        int dm = (di + dj) / 2;
-        if (m.yden[dm] > den) dj = dm; else di = dm;
+    if (m.yden_bkt) {
+        di = axis_search(den, m.yden, m.nden, m.yden_bkt, m.yden_nb, m.yden_b0, m.yden_binv);
+        dj = di + 1;
+    } else {
+        while (di + 1 < dj) {
+            int dm = (di + dj) / 2;
+            if (m.yden[dm] > den) dj = dm; else di = dm;
+        }
     }
     double dxr = (den - m.yden[di]) / (m.yden[dj] - m.yden[di]);
     dxr = wind(dxr, 0.0, 1.0);

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cctype>
 #include <cstddef>
 #include <cstdio>
@@ -220,6 +221,39 @@ int upload_vec(salec_gpu *h, const std::vector<T> &v, const T **out)
     return SALEC_OK;
 }
 
+// Bucket guesses for axis_search over xs[0..n-1]: 2n uniform buckets over [xs[0], xs[n-1]);
+// bucket b holds the largest k <= n-2 with xs[k] <= xs[0] + b * width. No table (false) for an
+// axis that is not non-decreasing and finite: the device then bisects.
+bool build_axis_buckets(const double *xs, int n, std::vector<int> &bkt, double &b0, double &binv)
+{
+    if (n < 3) return false;
+    for (int k = 0; k < n; ++k)
+        if (!std::isfinite(xs[k]) || (k && !(xs[k] >= xs[k - 1]))) return false;
+    const double span = xs[n - 1] - xs[0];
+    const int nb = 2 * n;
+    if (!(span > 0.0) || !std::isfinite(nb / span)) return false;
+    b0 = xs[0];
+    binv = nb / span;
+    bkt.resize(nb);
+    int k = 0;
+    for (int b = 0; b < nb; ++b) {
+        const double edge = xs[0] + b * (span / nb);
+        while (k < n - 2 && xs[k + 1] <= edge) ++k;
+        bkt[b] = k;
+    }
+    return true;
+}
+
+int upload_axis(salec_gpu *h, const double *xs, int n, const int **bkt, int *nb, double *b0, double *binv)
+{
+    std::vector<int> v;
+    *bkt = nullptr;
+    *nb = 0;
+    if (!build_axis_buckets(xs, n, v, *b0, *binv)) return SALEC_OK;
+    *nb = (int)v.size();
+    return upload_vec(h, v, bkt);
+}
+
 int make_gather(salec_gpu *h, Gather &g, const std::vector<std::pair<int, GatherMap>> &maps)
 {
     g = Gather();
@@ -318,7 +352,7 @@ int run_phase_t(salec_gpu *h, int ph)
     case 12:
         launch_step_kernel(SK_FLUX, c, s, h->blk[SK_FLUX], 0);
         rc = run_gather(h, h->g_flux_state);
-        launch_step_kernel(SK_FLUX, c, s, h->blk[SK_FLUX], 1);
+        launch_step_kernel(SK_FLUX, c, s, h->blk[SK_FLUX], (h->d.enx >= 5 && h->d.eny >= 5) ? 2 : 1);
         break;
     case 13:   // strength condition: count the lubricating tracers of every cell in e_cnd
         if (h->fork_tracers && h->tr.n > 0) CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));
@@ -416,6 +450,8 @@ int upload_material(salec_gpu *h, const salec_material_desc &m, DevMat &dm)
         if ((rc = upload_vec(h, x, &dm.xtem))) return rc;
         if ((rc = upload_vec(h, y, &dm.yden))) return rc;
         if ((rc = upload_vec(h, t, &dm.data))) return rc;
+        if ((rc = upload_axis(h, x.data(), m.ntem, &dm.xtem_bkt, &dm.xtem_nb, &dm.xtem_b0, &dm.xtem_binv))) return rc;
+        if ((rc = upload_axis(h, y.data(), m.nden, &dm.yden_bkt, &dm.yden_nb, &dm.yden_b0, &dm.yden_binv))) return rc;
     } else {
         return fail(SALEC_ERR_ARG, "unknown EOS type");
     }
@@ -1040,18 +1076,45 @@ int salec_gpu_phase_times(salec_gpu *h, double *ms, long long *count)
     return SALEC_OK;
 }
 
+namespace {
+// the 2-D sweep of each phase whose block shape is tunable
+const int kTunedPhase[] = {1, 3, 4, 5, 7, 8, 9, 10, 12, 14};
+const StepKernel kTunedKernel[] = {SK_VERTEX_VOF_MOMENTUM, SK_CELL_VELOCITY, SK_VOID_VERTICES, SK_GRADIENT,
+                                   SK_STRESS, SK_ACCELERATION, SK_DISPLACEMENT, SK_ENERGY, SK_FLUX,
+                                   SK_REMAP_DAMP_STATE};
+constexpr int kNumTuned = sizeof(kTunedPhase) / sizeof(kTunedPhase[0]);
+}   // namespace
+
+int salec_gpu_set_block_shapes(salec_gpu *h, const int *shapes, int n)
+{
+    if (!h || (n > 0 && !shapes) || n < 0) return fail(SALEC_ERR_ARG, "bad argument");
+    for (int k = 0; k < n; ++k) {
+        const int p = shapes[3 * k], bx = shapes[3 * k + 1], by = shapes[3 * k + 2];
+        int t = 0;
+        while (t < kNumTuned && kTunedPhase[t] != p) ++t;
+        if (t == kNumTuned) return fail(SALEC_ERR_ARG, "phase " + std::to_string(p) + " has no tunable block shape");
+        if (bx < 32 || bx % 32 || by < 1 || bx * by > 256)
+            return fail(SALEC_ERR_ARG, "block shape " + std::to_string(bx) + "x" + std::to_string(by) +
+                                           ": x must be a multiple of 32 and x*y at most 256");
+    }
+    for (int k = 0; k < n; ++k) {
+        int t = 0;
+        while (kTunedPhase[t] != shapes[3 * k]) ++t;
+        h->blk[kTunedKernel[t]] = dim3(shapes[3 * k + 1], shapes[3 * k + 2]);
+    }
+    if (h->cycle_graph) { cudaGraphExecDestroy(h->cycle_graph); h->cycle_graph = nullptr; }
+    return SALEC_OK;
+}
+
 int salec_gpu_autotune(salec_gpu *h, int cycles, int *shapes)
 {
     if (!h || cycles < 1) return fail(SALEC_ERR_ARG, "bad argument");
     static const dim3 cand[] = {dim3(32, 4), dim3(32, 8), dim3(64, 2), dim3(32, 2), dim3(64, 4), dim3(128, 1),
                                 dim3(32, 1), dim3(64, 1)};
     constexpr int ncand = sizeof(cand) / sizeof(cand[0]);
-    // the 2-D sweeps of each phase
-    static const int tuned_phase[] = {1, 3, 4, 5, 7, 8, 9, 10, 12, 14};
-    static const StepKernel tuned_kernel[] = {SK_VERTEX_VOF_MOMENTUM, SK_CELL_VELOCITY, SK_VOID_VERTICES, SK_GRADIENT,
-                                              SK_STRESS, SK_ACCELERATION, SK_DISPLACEMENT, SK_ENERGY, SK_FLUX,
-                                              SK_REMAP_DAMP_STATE};
-    constexpr int ntuned = sizeof(tuned_phase) / sizeof(tuned_phase[0]);
+    const int *tuned_phase = kTunedPhase;
+    const StepKernel *tuned_kernel = kTunedKernel;
+    constexpr int ntuned = kNumTuned;
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     // snapshot of everything the cycles change: the field pool, the scalars and the tracers
     void *snap = nullptr, *snap_tr = nullptr;

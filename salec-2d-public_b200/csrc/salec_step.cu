@@ -974,14 +974,37 @@ __device__ __forceinline__ void store_face(const CtxT<R> &c, double *f, double v
     }
 }
 
-// pass 0: interior cells; pass 1: pad cells (after the ghost fills of m_den, m_eng, ...).
+// Cell t of the two-cell pad ring, t < 4 enx + 4 (eny - 4): the two bottom rows, the two top
+// rows, then the four pad cells of each row between them (needs enx, eny >= 5).
+__device__ __forceinline__ void pad_ring_cell(int t, int enx, int eny, int &i, int &j)
+{
+    if (t < 2 * enx) {
+        j = t / enx; i = t - j * enx;
+    } else if (t < 4 * enx) {
+        const int u = t - 2 * enx, r = u / enx;
+        j = eny - 2 + r; i = u - r * enx;
+    } else {
+        const int u = t - 4 * enx, r = u >> 2, k = u & 3;
+        j = 2 + r; i = k < 2 ? k : enx - 4 + k;
+    }
+}
+
+// pass 0: interior cells; pass 1: pad cells (after the ghost fills of m_den, m_eng, ...), over
+// the whole grid; pass 2: the same pad cells, one thread each (1-D grid over the pad ring).
 template <class R, int NM, bool POR>
 __global__ void SALEC_BOUNDS_FLUX k_flux(const CtxT<R> c, int pass)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= c.d.enx || j >= c.d.eny) return;
-    const bool interior = cell_interior(c, i, j);
-    if ((pass == 0) != interior) return;
+    int i, j;
+    if (pass == 2) {
+        const int t = (blockIdx.x * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+        if (t >= 4 * c.d.enx + 4 * (c.d.eny - 4)) return;
+        pad_ring_cell(t, c.d.enx, c.d.eny, i, j);
+    } else {
+        i = blockIdx.x * blockDim.x + threadIdx.x;
+        j = blockIdx.y * blockDim.y + threadIdx.y;
+        if (i >= c.d.enx || j >= c.d.eny) return;
+        if ((pass == 0) != cell_interior(c, i, j)) return;
+    }
     constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
     const int nmat = NM > 0 ? NM : c.d.nmat;
     const long long p = KIDX(i, j);
@@ -1891,7 +1914,15 @@ void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, dim3 b, 
     case SK_TRACERS:
         if (c.tr.n > 0) k_tracers<R><<<(c.tr.n + 127) / 128, 128, 0, s>>>(c);
         break;
-    case SK_FLUX: SALEC_NM_DISPATCH(k_flux, c, a0); break;
+    case SK_FLUX:
+        if (a0 == 2) {   // pad ring, 1-D
+            const long long ring = 4LL * c.d.enx + 4LL * (c.d.eny - 4);
+            const dim3 g((unsigned)((ring + b.x * b.y - 1) / (b.x * b.y)));
+            SALEC_NM_DISPATCH(k_flux, c, a0);
+        } else {
+            SALEC_NM_DISPATCH(k_flux, c, a0);
+        }
+        break;
     case SK_REMAP_DAMP_STATE:
         // the pml3 remap is its own instance so that its extra state costs the others no registers
         if (c.rp.damp_type == 2) SALEC_NM_DISPATCH_P3(k_remap_damp_state, true, c, a0, a1, a2, a3);

@@ -85,6 +85,7 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_step": ([vp, c_i], c_i),
             "salec_gpu_step_many": ([ctypes.POINTER(vp), c_i, c_i, c_i], c_i),
             "salec_gpu_autotune": ([vp, c_i, ctypes.POINTER(c_i)], c_i),
+            "salec_gpu_set_block_shapes": ([vp, ctypes.POINTER(c_i), c_i], c_i),
             "salec_gpu_phases": ([vp, c_i, c_i], c_i),
             "salec_gpu_sync": ([vp], c_i),
             "salec_gpu_get_scalar": ([vp, ctypes.c_char_p, P_D], c_i),
@@ -317,6 +318,14 @@ class Simulation:
         out = (c_i * 30)()
         _check(lib().salec_gpu_autotune(self.h, int(cycles), out), "salec_gpu_autotune")
         return {out[3 * k]: (out[3 * k + 1], out[3 * k + 2]) for k in range(10)}
+
+    def set_block_shapes(self, shapes: dict) -> None:
+        """Set block shapes {phase: (block x, block y)} of tunable sweeps (as autotune returns)."""
+        items = sorted(shapes.items())
+        arr = (c_i * (3 * max(len(items), 1)))()
+        for k, (p, (bx, by)) in enumerate(items):
+            arr[3 * k], arr[3 * k + 1], arr[3 * k + 2] = int(p), int(bx), int(by)
+        _check(lib().salec_gpu_set_block_shapes(self.h, arr, len(items)), "salec_gpu_set_block_shapes")
 
     def check(self) -> int:
         n = c_ll()

@@ -30,3 +30,31 @@ def test_autotune_keeps_state_and_results(cuda_device, tmp_path):
     assert np.array_equal(a.get_tracers(), b.get_tracers())
     a.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_set_block_shapes_reuses_a_tuning(cuda_device, tmp_path):
+    """Shapes tuned on one handle, set on another of the same deck, change no result; invalid
+    triples are rejected as argument errors."""
+    deck = decks.write_deck(decks.Deck(npx=48, npy=64, radius_cells=5, damp_x=5, damp_y=5, velocity=-9000.0),
+                            str(tmp_path))
+    a = capi.Simulation.from_deck(deck, str(tmp_path))
+    b = capi.Simulation.from_deck(deck, str(tmp_path))
+    shapes = a.autotune(cycles=1)
+    odd = {ph: ((64, 4) if (bx, by) != (64, 4) else (32, 1)) for ph, (bx, by) in shapes.items()}
+    b.set_block_shapes(odd)
+    for bad in ({2: (32, 4)}, {7: (16, 2)}, {7: (32, 16)}, {7: (48, 1)}, {12: (32, 0)}):
+        with pytest.raises(capi.SalecError) as e:
+            b.set_block_shapes(bad)
+        assert e.value.code == -1
+    a.step(12)
+    b.step(12)
+    for n in fields.STATE_FIELDS:
+        assert np.array_equal(a.get_field(n), b.get_field(n), equal_nan=True), n
+    b.set_block_shapes(shapes)
+    a.step(5)
+    b.step(5)
+    for n in fields.STATE_FIELDS:
+        assert np.array_equal(a.get_field(n), b.get_field(n), equal_nan=True), n
+    a.close()
+    b.close()
