@@ -84,6 +84,19 @@ int ref_init_begin(const char *deck, const char *eosdir, const char *workdir)
         field_var *fv = g_sale.v_vel + k;
         if (fv->data) memset(fv->data, 0, (size_t)fv->data_size * fv->bytes_per_unit);
     }
+    /*
+     * A material without a porosity model (material.Porosity = None) never gets
+     * state_reference.alphamax2 (src/sale2d_back.c:369-395 sets it for Wunnemann only), yet a
+     * run with any porous material clamps the distension of every material to [1, alphamax2]
+     * (src/advect.c:272-277, src/sale2d.c:700-706). The clamp then reads heap garbage: a value
+     * >= 1 leaves the distension at 1, anything else writes the garbage into m_pty (and a NaN
+     * density later faults in TillTemp, src/eos/eos_state.c:521-524). Pin it to 1, the value
+     * that keeps a non-porous material at distension 1; the library's initialiser does the same.
+     */
+    for (int m = 1; m < g_sale.nmat; ++m) {
+        state_reference *r = g_sale.etb[m].ref;
+        if (r && strcasecmp(r->porosityfunc, "None") == 0) r->alphamax2 = 1.0;
+    }
     init_sale2d_other(&g_sale, g_ifp);
     init_sale2d_ghost(&g_sale, &g_minfo);
     CloseInputFile(g_ifp);

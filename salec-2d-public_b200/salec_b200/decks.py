@@ -403,6 +403,37 @@ def config2_deck(n: int = 2048, maxstep: int = 4999) -> Deck:
                 damping="pml", damp_x=30, damp_y=30, maxstep=maxstep, dt0=1.0e-4, maxdt=0.05)
 
 
+def config3_deck(n: int = 4096, maxstep: int = 2999, dx: float = 50.0, regolith: float = 500.0,
+                 basalt: float = 3000.0, cppr: float = 30.0, side_layers: int = 50, base_layers: int = 30) -> Deck:
+    """Layered three-material target, n x n cells: porous regolith (25% porosity, Wunnemann
+    compaction, cohesion 0.1 MPa) over basalt over a dunite half-space (Tillotson rho0 3320),
+    basalt projectile at CPPR 30 and 10 km/s. The reference has one damping type for the whole
+    mesh; its PML takes the side and base layer counts separately (DampX 50, DampY 30). The
+    seeded density noise of the configuration is applied to the initialised state by
+    density_noise()."""
+    regol = Material("regolit", poisson=0.25, yint0=1.0e5, yintfri=0.6, yintlim=1.0e9, ydam0=1.0e3,
+                     ydamfri=0.4, ydamlim=1.0e9, porosity="Wunnemann", alpha0=1.0 / 0.75, alphax=1.1,
+                     epse0=-1.0e-5, kappa=0.98, chi=0.5)
+    bas = Material("basalt_")
+    dun = Material("dunite_", poisson=0.28)
+    return Deck(npx=n, npy=n, dx=dx, dy=dx, oy=0.5, materials=[regol, bas, dun],
+                target_materials=["regolit", "basalt_", "dunite_"], target_depths=[regolith, basalt, 1.0e7],
+                projectile="basalt_", radius_cells=cppr, velocity=-10000.0, gravity=-1.62, damping="pml",
+                damp_x=side_layers, damp_y=base_layers, maxstep=maxstep, dt0=1.0e-4, maxdt=0.05)
+
+
+def density_noise(m_den: np.ndarray, e_den: np.ndarray, seed: int = 3, amplitude: float = 0.01):
+    """Seeded cell-by-cell noise of +-amplitude on the initial density field: every material
+    density of a cell and the cell density are scaled by the same factor 1 + amplitude * U(-1, 1),
+    drawn once per cell (the noise's correlation length is the cell size). Returns new arrays."""
+    rng = np.random.default_rng(seed)
+    f = 1.0 + amplitude * (2.0 * rng.random(e_den.shape[:2]) - 1.0)
+    md = m_den.copy()
+    md[..., 1:] *= f[..., None]
+    ed = e_den * f.reshape(e_den.shape[:2] + (1,) * (e_den.ndim - 2))
+    return md, ed
+
+
 def ensemble_decks(count: int = 256, seed: int = 2024, nmin: int = 128, nmax: int = 1024) -> List[Deck]:
     """Seeded ensemble of uneven impacts: grids drawn uniformly between nmin and nmax cells per
     axis, impactor speed U[5, 20] km/s, CPPR U{10..40}, cohesion log-uniform 1-100 MPa, friction

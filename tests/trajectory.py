@@ -136,6 +136,36 @@ def oracle_config_run(deck_fn: str, checkpoints: List[int], folder: str) -> Dict
     return out
 
 
+def oracle_noisy_deck_run(deck_kwargs: Dict, checkpoints: List[int], folder: str, seed: int,
+                          fields: List[str]) -> Dict:
+    """The reference's own initialisation of decks.config3_deck(**deck_kwargs), the seeded density
+    noise of decks.density_noise applied to its state, then its own time loop, recording
+    ``fields``, dt and time at each checkpoint cycle."""
+    d = bridge.decks.config3_deck(**deck_kwargs)
+    deck = bridge.decks.write_deck(d, folder)
+    ref.init(deck, folder, os.path.join(folder, "run"))
+    md, ed = bridge.decks.density_noise(ref.get("m_den"), ref.get("e_den"), seed=seed)
+    ref.set("m_den", md)
+    ref.set("e_den", ed)
+    out = {"deck": deck, "folder": folder, "at": {}}
+    done = 0
+    for k in checkpoints:
+        ref.step(k - done)
+        done = k
+        rec = {n: ref.get(n) for n in fields}
+        rec["dt"] = ref.scalar("dt")
+        rec["time"] = ref.scalar("time")
+        out["at"][k] = rec
+    return out
+
+
+def oracle_noisy_deck_run_isolated(deck_kwargs: Dict, checkpoints: List[int], folder: str, seed: int,
+                                   fields: List[str]) -> Dict:
+    ctx = mp.get_context("spawn")
+    with cf.ProcessPoolExecutor(max_workers=1, mp_context=ctx) as ex:
+        return ex.submit(oracle_noisy_deck_run, deck_kwargs, checkpoints, folder, seed, fields).result()
+
+
 def oracle_config_run_isolated(deck_fn: str, checkpoints: List[int], folder: str) -> Dict:
     ctx = mp.get_context("spawn")
     with cf.ProcessPoolExecutor(max_workers=1, mp_context=ctx) as ex:
