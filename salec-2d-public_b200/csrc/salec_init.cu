@@ -1604,9 +1604,30 @@ extern "C" int salec_gpu_create_from_deck_ex(const char *deck_path, const char *
     salec_gpu *h = nullptr;
     rc = salec_gpu_create(&run, mats.data(), &h);
     if (rc) return rc;
+    // The device pool starts zeroed (salec_gpu_create), so a field whose every value has the
+    // bits of +0.0 needs no upload. The scan runs on this thread, while uploads of concurrent
+    // initialisations serialise in the driver. Fields whose upload also builds device tables
+    // (geometry rows, the Laplacian mask) always go through salec_gpu_set_field.
+    auto all_plus_zero = [](const std::vector<double> &v) {
+        const unsigned long long *w = reinterpret_cast<const unsigned long long *>(v.data());
+        for (size_t k = 0; k < v.size(); k += 4096) {   // blocks of 32 KiB, early exit
+            const size_t e = std::min(v.size(), k + 4096);
+            unsigned long long acc = 0;
+            for (size_t j = k; j < e; ++j) acc |= w[j];
+            if (acc) return false;
+        }
+        return true;
+    };
+    static const char *const kTableFields[] = {"v_vol", "v_subvol", "v_suf", "e_grad", "e_vol", "v_laplace"};
     for (auto &kv : H.f) {
         int fid = salec_gpu_field_index(kv.first.c_str());
         if (fid < 0) continue;
+        bool tables = false;
+        for (const char *n : kTableFields) tables = tables || kv.first == n;
+        if (!tables && all_plus_zero(kv.second)) {
+            std::vector<double>().swap(kv.second);
+            continue;
+        }
         rc = salec_gpu_set_field(h, fid, kv.second.data(), (long long)kv.second.size());
         if (rc) { salec_gpu_destroy(h); return rc; }
         std::vector<double>().swap(kv.second);

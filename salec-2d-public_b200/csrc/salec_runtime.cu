@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -120,6 +121,11 @@ struct salec_gpu {
     Fields f{};
     DevMat *mat = nullptr;
     std::vector<void *> owned;   // device allocations besides the pool
+    // small device arrays of create (gather maps, EOS tables and their axis buckets): collected
+    // on the host by upload_vec and sent in one allocation and one copy by flush_uploads, so
+    // that creating a handle makes a few driver calls instead of one pair per array
+    std::vector<char> up_host;
+    std::vector<std::function<void(const char *)>> up_fix;
     Scal *scal = nullptr;
     Scal *scal_host = nullptr;   // pinned mirror
     double *scratch = nullptr;   // gather scratch
@@ -209,15 +215,32 @@ double *&field_ptr(salec_gpu *h, int k)
     return *reinterpret_cast<double **>(reinterpret_cast<char *>(&h->f) + kFields[k].off);
 }
 
+// Queue a host array for the device: *out receives its device address at the next
+// flush_uploads (null until then, and for an empty array).
 template <typename T>
 int upload_vec(salec_gpu *h, const std::vector<T> &v, const T **out)
 {
-    if (v.empty()) { *out = nullptr; return SALEC_OK; }
+    *out = nullptr;
+    if (v.empty()) return SALEC_OK;
+    const size_t off = (h->up_host.size() + 255) & ~(size_t)255;
+    h->up_host.resize(off + v.size() * sizeof(T));
+    memcpy(h->up_host.data() + off, v.data(), v.size() * sizeof(T));
+    h->up_fix.push_back([out, off](const char *base) { *out = reinterpret_cast<const T *>(base + off); });
+    return SALEC_OK;
+}
+
+// One device allocation for every queued array, one copy, then the addresses.
+int flush_uploads(salec_gpu *h)
+{
+    if (h->up_fix.empty()) return SALEC_OK;
     void *p = nullptr;
-    CUDA_TRY(cudaMalloc(&p, v.size() * sizeof(T)));
+    CUDA_TRY(cudaMalloc(&p, h->up_host.size()));
     h->owned.push_back(p);
-    CUDA_TRY(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
-    *out = static_cast<const T *>(p);
+    CUDA_TRY(cudaMemcpyAsync(p, h->up_host.data(), h->up_host.size(), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (auto &fix : h->up_fix) fix(static_cast<const char *>(p));
+    std::vector<char>().swap(h->up_host);
+    h->up_fix.clear();
     return SALEC_OK;
 }
 
@@ -530,16 +553,18 @@ int build_geo_table(salec_gpu *h, int slot, int fid, int nx, int ny, int nc)
     if (h->cycle_graph) { cudaGraphExecDestroy(h->cycle_graph); h->cycle_graph = nullptr; }
     const auto *src = reinterpret_cast<const unsigned long long *>(h->staging);
 
+    // temporaries are stream-ordered (cudaMallocAsync / cudaFreeAsync): freeing them does not
+    // synchronise the device, which would stall every other handle's work
     unsigned long long *d_hash = nullptr;
-    CUDA_TRY(cudaMalloc(&d_hash, sizeof(unsigned long long) * 2 * ny));
+    CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&d_hash), sizeof(unsigned long long) * 2 * ny, h->stream));
     k_geo_row_hash<<<ny, 256, 0, h->stream>>>(src, row_words, d_hash);
     cudaError_t e = cudaGetLastError();
     std::vector<unsigned long long> hashes(2 * (size_t)ny);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(hashes.data(), d_hash, sizeof(unsigned long long) * 2 * ny, cudaMemcpyDeviceToHost,
                             h->stream);
+    cudaFreeAsync(d_hash, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(d_hash);
     CUDA_TRY(e);
 
     // rows grouped in order of first appearance by their 128-bit hash
@@ -584,13 +609,15 @@ int build_geo_table(salec_gpu *h, int slot, int fid, int nx, int ny, int nc)
     unsigned *d_diff = nullptr;
     unsigned long long *d_rows = nullptr;   // the U distinct rows, AoS
     auto release_tmp = [&]() {
-        if (d_idx) cudaFree(d_idx);
-        if (d_diff) cudaFree(d_diff);
-        if (d_rows) cudaFree(d_rows);
+        if (d_idx) cudaFreeAsync(d_idx, h->stream);
+        if (d_diff) cudaFreeAsync(d_diff, h->stream);
+        if (d_rows) cudaFreeAsync(d_rows, h->stream);
     };
-    e = cudaMalloc(&d_idx, sizeof(int) * ((size_t)ny + U));
-    if (e == cudaSuccess) e = cudaMalloc(&d_diff, sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMalloc(&d_rows, sizeof(unsigned long long) * (size_t)U * row_words);
+    e = cudaMallocAsync(reinterpret_cast<void **>(&d_idx), sizeof(int) * ((size_t)ny + U), h->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void **>(&d_diff), sizeof(unsigned), h->stream);
+    if (e == cudaSuccess)
+        e = cudaMallocAsync(reinterpret_cast<void **>(&d_rows), sizeof(unsigned long long) * (size_t)U * row_words,
+                            h->stream);
     if (e == cudaSuccess) e = cudaMalloc(&g.tab, (size_t)nc * plane * field_elem(h, fid));
     if (e == cudaSuccess) e = cudaMalloc(&g.row, sizeof(int) * h->d.R);
     g.compact = true;
@@ -630,10 +657,11 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
     const long long need = (long long)nx * ny * nc;
     if (n != need) return fail(SALEC_ERR_ARG, std::string("field ") + kFields[fid].name + ": expected " +
                                                   std::to_string(need) + " doubles, got " + std::to_string(n));
-    if ((size_t)need > h->staging_doubles) {
-        if (h->staging) cudaFree(h->staging);
+    if ((size_t)need > h->staging_doubles) {   // stream-ordered: no device-wide synchronisation
+        if (h->staging) CUDA_TRY(cudaFreeAsync(h->staging, h->stream));
         h->staging = nullptr;
-        CUDA_TRY(cudaMalloc(&h->staging, need * sizeof(double)));
+        h->staging_doubles = 0;
+        CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&h->staging), need * sizeof(double), h->stream));
         h->staging_doubles = need;
     }
     void *base = field_ptr(h, fid);
@@ -882,6 +910,7 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
         int rc = upload_material(h, mats[m], dms[m]);
         if (rc) return bail(rc);
     }
+    if (int rc = flush_uploads(h)) return bail(rc);
     if (cudaMalloc(&h->mat, sizeof(DevMat) * d.nmat) != cudaSuccess) return bail(fail(SALEC_ERR_ALLOC, "materials"));
     if (cudaMemcpy(h->mat, dms.data(), sizeof(DevMat) * d.nmat, cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(SALEC_ERR_CUDA, "material upload"));
@@ -898,6 +927,7 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
 
     int rc = build_gathers(h);
     if (rc) return bail(rc);
+    if ((rc = flush_uploads(h))) return bail(rc);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(SALEC_ERR_CUDA, "create sync"));
     *out = h;
     return SALEC_OK;
