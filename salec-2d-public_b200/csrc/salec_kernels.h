@@ -19,7 +19,13 @@ struct GatherField {
     int f32;               // the field is stored as float
     const int *dst, *src;
     const unsigned *ops;
+    // null: one work item per entry. Otherwise entries are grouped into components (no point of
+    // a component is read or written by another) and work item w covers entries
+    // [cstart[w], cstart[w+1]), at most SALEC_GATHER_MAX_COMPONENT of them
+    const int *cstart;
 };
+
+constexpr int SALEC_GATHER_MAX_COMPONENT = 16;
 
 struct GatherBatch {
     GatherField field[SALEC_MAX_GATHER_FIELDS];

@@ -126,12 +126,26 @@ __global__ void k_trace_profile(const CtxT<R> c)
     const int j0 = blockIdx.y * 64 + threadIdx.y;
     unsigned long long best = ~0ULL;
     if (i < c.d.enx) {
-        for (int j = j0; j < min(c.d.eny, (int)blockIdx.y * 64 + 64); j += 8) {
-            long long p = KIDX(i, j);
-            double v0 = c.f.m_vof[p];
-            double y = PLN(c.f.e_pos, 1)[p];
-            if (v0 > 0.1) best = min(best, ord_encode(y));
-            if (y > c.rp.threshold_z && v0 < SALEC_TOLVOF) c.f.e_ejt[p] = 1.0;
+        // the thread's 8 rows are loaded before any is used, so that all 16 loads are in flight
+        // together; the MIN is order-independent
+        const int jend = min(c.d.eny, (int)blockIdx.y * 64 + 64);
+        double v0[8], y[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int j = j0 + 8 * k;
+            v0[k] = 0.0; y[k] = 0.0;
+            if (j < jend) {
+                const long long p = KIDX(i, j);
+                v0[k] = c.f.m_vof[p];
+                y[k] = PLN(c.f.e_pos, 1)[p];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int j = j0 + 8 * k;
+            if (j >= jend) continue;
+            if (v0[k] > 0.1) best = min(best, ord_encode(y[k]));
+            if (y[k] > c.rp.threshold_z && v0[k] < SALEC_TOLVOF) c.f.e_ejt[KIDX(i, j)] = 1.0;
         }
     }
     smin[threadIdx.y][threadIdx.x] = best;
@@ -1794,15 +1808,48 @@ __device__ __forceinline__ void gather_one(const GatherField &gf, int mode, long
     }
 }
 
+// One component of a map whose sources include destinations: per plane, every source of the
+// component is read before any destination is written, which is what the two passes through
+// scratch do for the whole map (the component's points are touched by no other thread, and
+// planes are disjoint).
+template <class T>
+__device__ __forceinline__ void gather_component(const GatherField &gf, int a, int b)
+{
+    T *base = static_cast<T *>(gf.base);
+    // fixed-length predicated loops: every load of the component is issued before the first
+    // one is needed
+    int src[SALEC_GATHER_MAX_COMPONENT], dst[SALEC_GATHER_MAX_COMPONENT];
+    unsigned ops[SALEC_GATHER_MAX_COMPONENT];
+#pragma unroll
+    for (int e = 0; e < SALEC_GATHER_MAX_COMPONENT; ++e)
+        if (a + e < b) { src[e] = gf.src[a + e]; dst[e] = gf.dst[a + e]; ops[e] = gf.ops[a + e]; }
+    for (int comp = 0; comp < gf.ncomp; ++comp) {
+        T *plane = base + (long long)comp * gf.plane;
+        double v[SALEC_GATHER_MAX_COMPONENT];
+#pragma unroll
+        for (int e = 0; e < SALEC_GATHER_MAX_COMPONENT; ++e)
+            if (a + e < b) v[e] = apply_op((ops[e] >> (3 * comp)) & 7u, (double)plane[src[e]]);
+#pragma unroll
+        for (int e = 0; e < SALEC_GATHER_MAX_COMPONENT; ++e)
+            if (a + e < b) plane[dst[e]] = (T)v[e];
+    }
+}
+
 __global__ void k_gather(GatherBatch g, int mode, double *scratch)
 {
-    // mode 0: in place; 1: gather into scratch; 2: scatter from scratch
+    // mode 0: in place, one entry (or one component, where the field has them) per thread;
+    // 1: gather into scratch; 2: scatter from scratch
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= g.total) return;
     int f = 0;
     while (f + 1 < g.nfield && t >= g.start[f + 1]) ++f;
     const GatherField &gf = g.field[f];
     const int k = t - g.start[f];
+    if (mode == 0 && gf.cstart) {
+        if (gf.f32) gather_component<float>(gf, gf.cstart[k], gf.cstart[k + 1]);
+        else gather_component<double>(gf, gf.cstart[k], gf.cstart[k + 1]);
+        return;
+    }
     if (gf.f32) gather_one<float>(gf, mode, gf.dst[k], gf.src[k], gf.ops[k], scratch, t);
     else gather_one<double>(gf, mode, gf.dst[k], gf.src[k], gf.ops[k], scratch, t);
 }
