@@ -213,30 +213,59 @@ def make_deck(n: int, folder: str) -> str:
 
 
 # ---------------------------------------------------------------- CPU reference leg
-def cpu_reference(n: int, steps: int, warmup: int, folder: str, gpu_state=None):
-    """Time the reference's own step loop (oracle/_ref) on an n x n sample of the workload.
-
-    The reference starts from the state the GPU arm starts from: its geometry comes from its
-    own init_mesh_pos, every field is then set from the deck initialiser's state (the
-    reference's own target-profile search over the 512 x 512 table would take minutes).
-    """
+def _cpu_reference_worker(state_path: str, n: int, steps: int, warmup: int, barrier, results) -> None:
+    """One reference process of cpu_reference_cores: its own oracle instance (the reference
+    keeps global state), its own copy of the sample, timed between a common barrier and its
+    own end."""
     from oracle import ref
-    cwd = os.getcwd()
+    folder = tempfile.mkdtemp(prefix="salec_cpu_")
+    st = np.load(state_path)
     deck = make_deck(n, folder)
-    sim = capi.Simulation.from_deck(deck, folder) if gpu_state is None else None
     ref.init(deck, folder, os.path.join(folder, "run"), material=False)
     for name in fields.STEP_FIELDS:
-        ref.set(name, sim.get_field(name) if sim is not None else gpu_state[name])
-    damp = sim.get_run().damp_time if sim is not None else gpu_state["damp_time"]
-    if sim is not None:
-        sim.close()
-    ref.init_adopt(damp)
+        ref.set(name, st[name])
+    ref.init_adopt(float(st["damp_time"]))
     ref.step(warmup)
+    barrier.wait()
     t0 = time.perf_counter()
     ref.step(steps)
-    dt = time.perf_counter() - t0
-    os.chdir(cwd)   # the oracle works in its own folder
-    return n * n * steps / dt, dt
+    results.put(time.perf_counter() - t0)
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_reference_cores(n: int, steps: int, warmup: int, folder: str, procs: int):
+    """The reference on every host core: the reference is an MPI code, single-threaded per rank,
+    and the one-rank shim cannot split a domain, so each core runs its own reference process on
+    its own n x n copy of the workload (the throughput an MPI run of procs ranks could reach at
+    best, with no halo exchange). All start from the library's deck-initialised state (bit-equal
+    to the reference's own init), step `warmup` cycles, meet at a barrier and step `steps`
+    cycles; the rate is procs x n^2 x steps over the slowest process's time."""
+    import multiprocessing as mp
+    deck = make_deck(n, folder)
+    sim = capi.Simulation.from_deck(deck, folder)
+    state = {name: sim.get_field(name) for name in fields.STEP_FIELDS}
+    state["damp_time"] = np.array(sim.get_run().damp_time)
+    sim.close()
+    path = os.path.join(folder, "cpu_state.npz")
+    np.savez(path, **state)
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs)
+    results = ctx.Queue()
+    workers = [ctx.Process(target=_cpu_reference_worker, args=(path, n, steps, warmup, barrier, results))
+               for _ in range(procs)]
+    for w in workers:
+        w.start()
+    times = [results.get(timeout=3600) for _ in workers]
+    for w in workers:
+        w.join()
+    secs = max(times)
+    return procs * n * n * steps / secs, secs
 
 
 def run_reference_arm(args):
@@ -244,15 +273,18 @@ def run_reference_arm(args):
     if rank != 0:
         return
     n = args.cpu_n
+    procs = host_cores()
     with tempfile.TemporaryDirectory() as tmp:
-        rate, secs = cpu_reference(n, args.steps, args.warmup, tmp)
+        rate, secs = cpu_reference_cores(n, args.steps, args.warmup, tmp, procs)
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "cell-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload(args.n), "sample": "%dx%d cells of the same deck" % (n, n),
-                       "parallelism": "single host thread (the reference is single-threaded per rank)"},
-            "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                             "sample": "%d steps of a %dx%d-cell copy of the workload" % (args.steps, n, n)},
+                       "parallelism": "%d reference processes, one per host core, each on its own copy "
+                                      "(single-threaded per rank, no halo exchange)" % procs},
+            "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
+                             "sample": "%d steps of a %dx%d-cell copy of the workload on each of %d processes"
+                                       % (args.steps, n, n, procs)},
             "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -483,11 +515,12 @@ def run_gpu_arm(args):
 
     cpu = None
     if rank == 0 and not args.no_cpu:
+        procs = host_cores()
         with tempfile.TemporaryDirectory() as ctmp:
-            rate, secs = cpu_reference(args.cpu_n, args.cpu_steps, 2, ctmp)
-        cpu = {"value": rate, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-               "sample": "%d steps of a %dx%d-cell copy of the workload (%.1f s)" % (args.cpu_steps, args.cpu_n,
-                                                                                   args.cpu_n, secs)}
+            rate, secs = cpu_reference_cores(args.cpu_n, args.cpu_steps, 2, ctmp, procs)
+        cpu = {"value": rate, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
+               "sample": "%d steps of a %dx%d-cell copy of the workload on each of %d reference processes, "
+                         "one per host core (%.1f s)" % (args.cpu_steps, args.cpu_n, args.cpu_n, procs, secs)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
