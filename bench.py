@@ -195,10 +195,30 @@ def rel_l2(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
 
 
-def crater_depth(profile: np.ndarray, surface: float, ncols: int = 4) -> float:
-    """Transient crater depth from the surface profile: the lowest surface height over the
-    columns next to the symmetry axis, below the pre-impact surface."""
-    return float(surface - np.min(profile[2:2 + ncols]))
+def dense_top(e_den: np.ndarray, e_pos: np.ndarray, rho: float) -> np.ndarray:
+    """Per interior column, the height where the density falls through rho above the highest
+    cell at least that dense, interpolated linearly between that cell's centre and the next one
+    up (NaN where no cell is that dense). Arrays in the reference layout (rows, columns,
+    components)."""
+    den = e_den[2:-2, 2:-2, 0]
+    y = e_pos[2:-2, 2:-2, 1]
+    rows = np.arange(den.shape[0])[:, None]
+    k = np.where(den >= rho, rows, -1).max(axis=0)            # highest dense row per column
+    cols = np.arange(den.shape[1])
+    ok = k >= 0
+    kk = np.clip(k, 0, den.shape[0] - 1)
+    k1 = np.clip(kk + 1, 0, den.shape[0] - 1)
+    d0, d1 = den[kk, cols], den[k1, cols]
+    y0, y1 = y[kk, cols], y[k1, cols]
+    frac = np.where((k1 > kk) & (d0 > d1), (d0 - rho) / np.where(d0 > d1, d0 - d1, 1.0), 0.0)
+    return np.where(ok, y0 + frac * (y1 - y0), np.nan)
+
+
+def crater_depth(e_den: np.ndarray, e_pos: np.ndarray, rho: float, surface: float) -> float:
+    """Transient crater depth on the symmetry axis: the pre-impact surface height minus the top
+    of the dense target (density >= rho, half the target's) in the column next to the axis. The
+    vaporised plume above the floor is far less dense, so it does not count as surface."""
+    return float(surface - dense_top(e_den, e_pos, rho)[0])
 
 
 def dist_setup():
@@ -487,7 +507,6 @@ def run_gpu_arm(args):
         sim.step(args.warmup + args.steps)
         fields_cmp = ("e_den", "e_pre", "m_eng", "m_vof", "v_vel")
         ref_state = {n: sim.get_field(n) for n in fields_cmp}
-        ref_profile = sim.get_field("y_profile").reshape(-1)
         errs = {n: rel_l2(mix.get_field(n), ref_state[n]) for n in fields_cmp}
         # sensitivity of the FP64 form itself: the same run with m_den and m_eng perturbed by 1e-7
         # relative at the start (the size of one FP32 rounding)
@@ -498,19 +517,53 @@ def run_gpu_arm(args):
         sim.set_scalar("time", 0.0)
         sim.step(args.warmup + args.steps)
         sens = {n: rel_l2(sim.get_field(n), ref_state[n]) for n in fields_cmp}
-        prof64 = ref_profile
-        surface = float(np.median(prof64[2:-2]))   # most columns are still at the pre-impact surface
-        d64 = crater_depth(prof64, surface)
-        d32 = crater_depth(mix.get_field("y_profile").reshape(-1), surface)
+        den0 = init_state["e_den"]
+        rho_half = 0.5 * float(np.median(den0[den0 > 0.0]))    # half the target's density
+        surface = float(np.nanmedian(dense_top(den0, init_state["e_pos"], rho_half)))
+        d64 = crater_depth(ref_state["e_den"], init_state["e_pos"], rho_half, surface)
+        d32 = crater_depth(mix.get_field("e_den"), init_state["e_pos"], rho_half, surface)
         mixed = {"value": mvalue, "unit": "cell-updates/s", "ms_per_step": mms / args.steps,
                  "speedup_vs_fp64": mvalue / value,
                  "storage": "FP32 relaxed fields, FP64 m_vof/m_den/m_eng/m_pty/e_cvs/positions/volumes/face records",
                  "arithmetic": "f64",
                  "rel_l2_vs_fp64": errs, "cycles_compared": args.warmup + args.steps,
                  "fp64_sensitivity_rel_l2": sens,
-                 "crater_depth_m": {"fp64": max(d64, 0.0), "mixed": max(d32, 0.0),
-                                    "rel_err": abs(d32 - d64) / d64 if d64 > 0 else None},
+                 "crater_depth_m": {"fp64": d64, "mixed": d32,
+                                    "rel_err": abs(d32 - d64) / d64 if d64 > 0 else None,
+                                    "measure": "surface minus the top of density >= %.0f kg/m3 on the axis" % rho_half},
                  "nonfinite": mix.check()}
+        # the configured run length: both forms from the start to --long-cycles (untimed), then
+        # field errors and the transient crater depth of each
+        total = args.warmup + args.steps
+        if args.long_cycles > total:
+            mix.step(args.long_cycles - total)
+            for name, a in init_state.items():
+                sim.set_field(name, a)
+            sim.set_tracers(init_tracers)
+            sim.set_scalar("dt", run.dt)
+            sim.set_scalar("time", 0.0)
+            sim.step(args.long_cycles)
+            l64 = crater_depth(sim.get_field("e_den"), init_state["e_pos"], rho_half, surface)
+            l32 = crater_depth(mix.get_field("e_den"), init_state["e_pos"], rho_half, surface)
+            long64 = {n: sim.get_field(n) for n in fields_cmp}
+            long_t, bad = sim.scalar("time"), mix.check() + sim.check()
+            long_mix = {n: rel_l2(mix.get_field(n), long64[n]) for n in fields_cmp}
+            # the FP64 form's own sensitivity over the same run: m_den, m_eng perturbed by 1e-7
+            for name, a in init_state.items():
+                sim.set_field(name, a * (1.0 + 1e-7) if name in ("m_den", "m_eng") else a)
+            sim.set_tracers(init_tracers)
+            sim.set_scalar("dt", run.dt)
+            sim.set_scalar("time", 0.0)
+            sim.step(args.long_cycles)
+            lp = crater_depth(sim.get_field("e_den"), init_state["e_pos"], rho_half, surface)
+            mixed["long_run"] = {
+                "cycles": args.long_cycles, "time_s": long_t,
+                "rel_l2_vs_fp64": long_mix,
+                "fp64_sensitivity_rel_l2": {n: rel_l2(sim.get_field(n), long64[n]) for n in fields_cmp},
+                "crater_depth_m": {"fp64": l64, "mixed": l32, "fp64_perturbed": lp,
+                                   "rel_err": abs(l32 - l64) / l64 if l64 > 0 else None,
+                                   "fp64_sensitivity_rel": abs(lp - l64) / l64 if l64 > 0 else None},
+                "nonfinite": bad + sim.check()}
         mix.close()
 
     cpu = None
@@ -707,6 +760,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
+    ap.add_argument("--long-cycles", type=int, default=5000,
+                    help="cycles of the mixed-vs-FP64 accuracy run at the configured length (0: skip)")
     ap.add_argument("--ensemble", type=int, default=0, help="run the ensemble mode with this many members")
     ap.add_argument("--ens-steps", type=int, default=2000)
     ap.add_argument("--ens-chunk", type=int, default=32)
