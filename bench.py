@@ -9,8 +9,13 @@ energy) EOS, ice Tillotson projectile at CPPR 40 and 15 km/s, rock strength with
 Arms:
   default          the GPU library through its C ABI (include/salec_gpu.h)
   --impl reference the reference's own CPU step loop (the compiled reference in
-                   oracle/_ref, single-threaded as the reference is), timed on a bounded
-                   sample of the same workload
+                   oracle/_ref, one single-threaded reference process per host core, each on
+                   its own bounded copy of the same workload, aggregate over a common window)
+
+The default line also carries the mixed form (speed, and its accuracy against the FP64 form
+after the timed cycles and after the configured 5000 cycles, with the transient crater depth),
+the roofline of the dominant kernel, the end-to-end figure through host buffers and the CPU
+baseline. --layered and --ensemble N run the layered-target and ensemble workloads instead.
 
 Multi-GPU (torchrun): independent replicas, one simulation per GPU, no collective on the
 data path; the reported value is the total over all ranks with the max-over-ranks time.
