@@ -48,38 +48,61 @@ namespace salec {
 #ifndef SALEC_REGS_ENERGY
 #define SALEC_REGS_ENERGY 40
 #endif
+// budgets of the mixed form's instances (relaxed fields stored as float), SALEC_REGS_<K>_F,
+// measured the same way on the mixed form of the same workload
+#ifndef SALEC_REGS_STRESS_F
+#define SALEC_REGS_STRESS_F SALEC_REGS_STRESS
+#endif
+#ifndef SALEC_REGS_FLUX_F
+#define SALEC_REGS_FLUX_F SALEC_REGS_FLUX
+#endif
+#ifndef SALEC_REGS_REMAP_F
+#define SALEC_REGS_REMAP_F 88
+#endif
+#ifndef SALEC_REGS_ENERGY_F
+#define SALEC_REGS_ENERGY_F 32
+#endif
+#ifndef SALEC_REGS_ACCEL_F
+#define SALEC_REGS_ACCEL_F 56
+#endif
+#ifndef SALEC_REGS_VOFMOM_F
+#define SALEC_REGS_VOFMOM_F SALEC_REGS_VOFMOM
+#endif
+#ifndef SALEC_REGS_GRAD_F
+#define SALEC_REGS_GRAD_F SALEC_REGS_GRAD
+#endif
 #if SALEC_REGS_STRESS > 0
-#define SALEC_BOUNDS_STRESS __maxnreg__(SALEC_REGS_STRESS)
+#define SALEC_BOUNDS_STRESS __maxnreg__((sizeof(R) == 4 ? SALEC_REGS_STRESS_F : SALEC_REGS_STRESS))
 #else
 #define SALEC_BOUNDS_STRESS __launch_bounds__(256)
 #endif
 #if SALEC_REGS_FLUX > 0
-#define SALEC_BOUNDS_FLUX __maxnreg__(SALEC_REGS_FLUX)
+#define SALEC_BOUNDS_FLUX __maxnreg__((sizeof(R) == 4 ? SALEC_REGS_FLUX_F : SALEC_REGS_FLUX))
 #else
 #define SALEC_BOUNDS_FLUX __launch_bounds__(256)
 #endif
 #if SALEC_REGS_REMAP > 0
-#define SALEC_BOUNDS_REMAP __maxnreg__(SALEC_REGS_REMAP)
+#define SALEC_BOUNDS_REMAP __maxnreg__((sizeof(R) == 4 ? SALEC_REGS_REMAP_F : SALEC_REGS_REMAP))
 #else
 #define SALEC_BOUNDS_REMAP __launch_bounds__(256)
 #endif
 #if SALEC_REGS_ENERGY > 0
-#define SALEC_BOUNDS_ENERGY __maxnreg__(SALEC_REGS_ENERGY)
+#define SALEC_BOUNDS_ENERGY __maxnreg__((sizeof(R) == 4 ? SALEC_REGS_ENERGY_F : SALEC_REGS_ENERGY))
 #else
 #define SALEC_BOUNDS_ENERGY __launch_bounds__(256)
 #endif
 #if SALEC_REGS_ACCEL > 0
-#define SALEC_BOUNDS_ACCEL __maxnreg__(SALEC_REGS_ACCEL)
+#define SALEC_BOUNDS_ACCEL __maxnreg__((sizeof(R) == 4 ? SALEC_REGS_ACCEL_F : SALEC_REGS_ACCEL))
 #else
 #define SALEC_BOUNDS_ACCEL
 #endif
 #if SALEC_REGS_VOFMOM > 0
-#define SALEC_BOUNDS_VOFMOM __maxnreg__(SALEC_REGS_VOFMOM)
+#define SALEC_BOUNDS_VOFMOM __maxnreg__((sizeof(R) == 4 ? SALEC_REGS_VOFMOM_F : SALEC_REGS_VOFMOM))
 #else
 #define SALEC_BOUNDS_VOFMOM
 #endif
 #if SALEC_REGS_GRAD > 0
-#define SALEC_BOUNDS_GRAD __maxnreg__(SALEC_REGS_GRAD)
+#define SALEC_BOUNDS_GRAD __maxnreg__((sizeof(R) == 4 ? SALEC_REGS_GRAD_F : SALEC_REGS_GRAD))
 #else
 #define SALEC_BOUNDS_GRAD
 #endif
