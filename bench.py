@@ -459,7 +459,7 @@ def run_gpu_arm(args):
     sim.set_scalar("time", 0.0)
     out_fields = fields.OUTPUT_FIELDS
     h2d = sum(a.nbytes for a in init_state.values()) + init_tracers.nbytes
-    d2h_step = 8 * 2 + 8 * (n + 4)
+    d2h_step = 48 + 8 * (n + 4)   # the 48-byte scalar block (dt, time, ...) and the surface profile
     d2h_out = sum(8 * np.prod(sim.shape(f)) for f in out_fields)
     out_bufs = {f: torch.empty(int(np.prod(sim.shape(f))), dtype=torch.float64, pin_memory=True).numpy()
                 .reshape(sim.shape(f)) for f in out_fields}
@@ -474,10 +474,7 @@ def run_gpu_arm(args):
     sim.set_scalar("dt", run.dt)
     t_up = time.perf_counter()
     for _ in range(args.steps):
-        sim.step(1)
-        sim.scalar("dt")
-        sim.scalar("time")
-        sim.get_field("y_profile", out=prof_buf)
+        sim.step_report(1, prof_buf)   # the cycle, then dt, time and the surface profile
     t_loop = time.perf_counter()
     outs = [sim.get_field(f, out=out_bufs[f]) for f in out_fields]
     sim.sync()

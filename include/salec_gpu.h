@@ -146,6 +146,13 @@ int salec_gpu_get_field(salec_gpu *h, int field, double *host, long long n);
 
 /* Advance nsteps full cycles: the loop body of src/salec2d.c:115-272 without the output point. */
 int salec_gpu_step(salec_gpu *h, int nsteps);
+/* salec_gpu_step, then the per-cycle quantities of the reference's loop: dt and the simulated
+ * time (the MIN-reduced ccl.dt and ccl.step_time, src/salec2d.c:167-168; either pointer may be
+ * NULL) and, when profile is not NULL, the surface profile y_profile (the MIN-reduced
+ * sale2d.y_profile, src/salec2d.c:120, 232; profile_n doubles, its field shape). The read-backs are queued
+ * behind the cycles and the call synchronises once, where salec_gpu_get_scalar and
+ * salec_gpu_get_field would synchronise once each. Results equal those calls'. */
+int salec_gpu_step_report(salec_gpu *h, int nsteps, double *dt, double *time, double *profile, long long profile_n);
 /* Advance an ensemble of independent simulations (each handle a different deck or mesh size)
  * by nsteps cycles each. Cycles are queued round-robin, chunk cycles per member at a time, each
  * member on its own stream, so the kernels of small meshes run side by side on the device.

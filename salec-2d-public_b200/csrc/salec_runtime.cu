@@ -708,6 +708,18 @@ int build_geo_table(salec_gpu *h, int slot, int fid, int nx, int ny, int nc)
     return SALEC_OK;
 }
 
+// AoS staging buffer of at least `need` doubles (stream-ordered: no device-wide synchronisation)
+int ensure_staging(salec_gpu *h, size_t need)
+{
+    if (need <= h->staging_doubles) return SALEC_OK;
+    if (h->staging) CUDA_TRY(cudaFreeAsync(h->staging, h->stream));
+    h->staging = nullptr;
+    h->staging_doubles = 0;
+    CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&h->staging), need * sizeof(double), h->stream));
+    h->staging_doubles = need;
+    return SALEC_OK;
+}
+
 int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
 {
     if (fid < 0 || fid >= kNumFields) return fail(SALEC_ERR_ARG, "unknown field");
@@ -717,13 +729,7 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
     const long long need = (long long)nx * ny * nc;
     if (n != need) return fail(SALEC_ERR_ARG, std::string("field ") + kFields[fid].name + ": expected " +
                                                   std::to_string(need) + " doubles, got " + std::to_string(n));
-    if ((size_t)need > h->staging_doubles) {   // stream-ordered: no device-wide synchronisation
-        if (h->staging) CUDA_TRY(cudaFreeAsync(h->staging, h->stream));
-        h->staging = nullptr;
-        h->staging_doubles = 0;
-        CUDA_TRY(cudaMallocAsync(reinterpret_cast<void **>(&h->staging), need * sizeof(double), h->stream));
-        h->staging_doubles = need;
-    }
+    if (int rc = ensure_staging(h, (size_t)need)) return rc;
     void *base = field_ptr(h, fid);
     const bool f32 = field_f32(h, fid);
     const long long plane = kFields[fid].loc == L_COL ? 0 : h->d.PL;
@@ -1115,6 +1121,35 @@ int salec_gpu_step(salec_gpu *h, int nsteps)
             if (rc) return rc;
         }
     }
+    return SALEC_OK;
+}
+
+int salec_gpu_step_report(salec_gpu *h, int nsteps, double *dt, double *time, double *profile, long long profile_n)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    const int fid = field_by_name("y_profile");
+    int nx = 0, ny = 0;
+    field_points(h, fid, nx, ny);
+    const long long need = (long long)nx * ny * field_ncomp(h, fid);
+    if (profile && profile_n != need)
+        return fail(SALEC_ERR_ARG, "y_profile: expected " + std::to_string(need) + " doubles, got " +
+                                       std::to_string(profile_n));
+    if (profile) {
+        if (int rc = ensure_staging(h, (size_t)need)) return rc;
+    }
+    if (int rc = salec_gpu_step(h, nsteps)) return rc;
+    // both read-backs queue behind the cycles; one synchronisation for all of them
+    CUDA_TRY(cudaMemcpyAsync(h->scal_host, h->scal, sizeof(Scal), cudaMemcpyDeviceToHost, h->stream));
+    if (profile) {
+        const long long plane = kFields[fid].loc == L_COL ? 0 : h->d.PL;
+        launch_planes_to_aos(field_ptr(h, fid), field_f32(h, fid), h->staging, plane, h->d.P, nx, ny,
+                             field_ncomp(h, fid), h->stream);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(profile, h->staging, need * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (dt) *dt = h->scal_host->dt;
+    if (time) *time = h->scal_host->time;
     return SALEC_OK;
 }
 

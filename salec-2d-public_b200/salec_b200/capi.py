@@ -84,6 +84,7 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_get_field": ([vp, c_i, P_D, c_ll], c_i),
             "salec_gpu_step": ([vp, c_i], c_i),
             "salec_gpu_step_many": ([ctypes.POINTER(vp), c_i, c_i, c_i], c_i),
+            "salec_gpu_step_report": ([vp, c_i, P_D, P_D, P_D, c_ll], c_i),
             "salec_gpu_autotune": ([vp, c_i, ctypes.POINTER(c_i)], c_i),
             "salec_gpu_set_block_shapes": ([vp, ctypes.POINTER(c_i), c_i], c_i),
             "salec_gpu_phases": ([vp, c_i, c_i], c_i),
@@ -285,6 +286,20 @@ class Simulation:
 
     def step(self, n: int = 1) -> None:
         _check(lib().salec_gpu_step(self.h, n), "step")
+
+    def step_report(self, n: int = 1, profile: np.ndarray | None = None):
+        """step(n), then (dt, time), and the surface profile into `profile` when given (a
+        C-contiguous float64 array of y_profile's shape), with one synchronisation."""
+        dt, t = c_d(), c_d()
+        pp, pn = None, 0
+        if profile is not None:
+            shp = self.shape("y_profile")
+            if profile.dtype != np.float64 or tuple(profile.shape) != tuple(shp) or not profile.flags.c_contiguous:
+                raise ValueError("step_report: profile must be C-contiguous float64 of shape %s" % (shp,))
+            pp, pn = _ptr(profile), profile.size
+        _check(lib().salec_gpu_step_report(self.h, int(n), ctypes.byref(dt), ctypes.byref(t), pp, pn),
+               "step_report")
+        return dt.value, t.value
 
     def phases(self, first: int, last: int) -> None:
         _check(lib().salec_gpu_phases(self.h, first, last), "phases")
