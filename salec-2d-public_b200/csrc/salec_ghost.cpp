@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <unordered_map>
 
 namespace salec {
 
@@ -258,6 +259,58 @@ GatherMap build_restrict_map(int vnx, int vny, int P, int ncomp, const int go[4]
         }
     }
     return rp.finish();
+}
+
+// Entries of a map whose sources include destinations, grouped into connected components of
+// the read/write relation (union of each entry's destination and source point), components in
+// order of their first entry and entries in map order within each; false when a component has
+// more than SALEC_GATHER_MAX_COMPONENT entries.
+bool group_gather_components(const GatherMap &m, GatherMap &out, std::vector<int> &cstart)
+{
+    std::unordered_map<int, int> id;
+    std::vector<int> parent;
+    auto node = [&](int pt) {
+        auto it = id.find(pt);
+        if (it != id.end()) return it->second;
+        const int n = (int)parent.size();
+        id.emplace(pt, n);
+        parent.push_back(n);
+        return n;
+    };
+    auto root = [&](int x) {
+        while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; }
+        return x;
+    };
+    const size_t ne = m.dst.size();
+    std::vector<int> en(ne);
+    for (size_t e = 0; e < ne; ++e) {
+        const int a = root(node(m.dst[e])), b = root(node(m.src[e]));
+        if (a != b) parent[a] = b;
+        en[e] = node(m.dst[e]);
+    }
+    std::unordered_map<int, int> comp_of;   // root -> component number (first-entry order)
+    std::vector<std::vector<int>> comps;
+    for (size_t e = 0; e < ne; ++e) {
+        const int r = root(en[e]);
+        auto it = comp_of.find(r);
+        if (it == comp_of.end()) {
+            it = comp_of.emplace(r, (int)comps.size()).first;
+            comps.emplace_back();
+        }
+        comps[it->second].push_back((int)e);
+        if ((int)comps[it->second].size() > SALEC_GATHER_MAX_COMPONENT) return false;
+    }
+    out = GatherMap();
+    cstart.assign(1, 0);
+    for (const auto &c : comps) {
+        for (int e : c) {
+            out.dst.push_back(m.dst[e]);
+            out.src.push_back(m.src[e]);
+            out.ops.push_back(m.ops[e]);
+        }
+        cstart.push_back((int)out.dst.size());
+    }
+    return true;
 }
 
 } // namespace salec

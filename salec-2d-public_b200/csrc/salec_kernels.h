@@ -49,6 +49,10 @@ GatherMap build_ghost_map(int enx, int eny, int P, int ncomp, const int go[4], G
 // Build the gather map of the vertex restriction table (vnx x vny points, pitch P).
 GatherMap build_restrict_map(int vnx, int vny, int P, int ncomp, const int go[4]);
 
+// Entries of a map whose sources include destinations, grouped into connected components of the
+// read/write relation; false when a component exceeds SALEC_GATHER_MAX_COMPONENT entries.
+bool group_gather_components(const GatherMap &m, GatherMap &out, std::vector<int> &cstart);
+
 // Step kernels of salec_step.cu, launched over their own grids by launch_step_kernel; R is
 // the storage type of the relaxed fields (double: plain FP64 form, float: mixed form).
 enum StepKernel {

@@ -277,58 +277,6 @@ int upload_axis(salec_gpu *h, const double *xs, int n, const int **bkt, int *nb,
     return upload_vec(h, v, bkt);
 }
 
-// Entries of a map whose sources include destinations, grouped into connected components of
-// the read/write relation (union of each entry's destination and source point), components in
-// order of their first entry and entries in map order within each; false when a component has
-// more than SALEC_GATHER_MAX_COMPONENT entries.
-bool group_components(const GatherMap &m, GatherMap &out, std::vector<int> &cstart)
-{
-    std::unordered_map<int, int> id;
-    std::vector<int> parent;
-    auto node = [&](int pt) {
-        auto it = id.find(pt);
-        if (it != id.end()) return it->second;
-        const int n = (int)parent.size();
-        id.emplace(pt, n);
-        parent.push_back(n);
-        return n;
-    };
-    auto root = [&](int x) {
-        while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; }
-        return x;
-    };
-    const size_t ne = m.dst.size();
-    std::vector<int> en(ne);
-    for (size_t e = 0; e < ne; ++e) {
-        const int a = root(node(m.dst[e])), b = root(node(m.src[e]));
-        if (a != b) parent[a] = b;
-        en[e] = node(m.dst[e]);
-    }
-    std::unordered_map<int, int> comp_of;   // root -> component number (first-entry order)
-    std::vector<std::vector<int>> comps;
-    for (size_t e = 0; e < ne; ++e) {
-        const int r = root(en[e]);
-        auto it = comp_of.find(r);
-        if (it == comp_of.end()) {
-            it = comp_of.emplace(r, (int)comps.size()).first;
-            comps.emplace_back();
-        }
-        comps[it->second].push_back((int)e);
-        if ((int)comps[it->second].size() > SALEC_GATHER_MAX_COMPONENT) return false;
-    }
-    out = GatherMap();
-    cstart.assign(1, 0);
-    for (const auto &c : comps) {
-        for (int e : c) {
-            out.dst.push_back(m.dst[e]);
-            out.src.push_back(m.src[e]);
-            out.ops.push_back(m.ops[e]);
-        }
-        cstart.push_back((int)out.dst.size());
-    }
-    return true;
-}
-
 int make_gather(salec_gpu *h, Gather &g, const std::vector<std::pair<int, GatherMap>> &maps)
 {
     g = Gather();
@@ -340,7 +288,8 @@ int make_gather(salec_gpu *h, Gather &g, const std::vector<std::pair<int, Gather
     std::vector<GatherMap> grouped(maps.size());
     std::vector<std::vector<int>> cstart(maps.size());
     for (size_t k = 0; k < maps.size() && !g.two_pass; ++k)
-        if (maps[k].second.needs_scratch && !group_components(maps[k].second, grouped[k], cstart[k])) g.two_pass = true;
+        if (maps[k].second.needs_scratch && !group_gather_components(maps[k].second, grouped[k], cstart[k]))
+            g.two_pass = true;
     for (size_t k = 0; k < maps.size(); ++k) {
         const int fid = maps[k].first;
         const bool comp = !g.two_pass && maps[k].second.needs_scratch;
