@@ -13,8 +13,10 @@
 // library is compiled with --fmad=false) so that the FP64 form reproduces the reference's
 // rounding wherever the math library allows.
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 #define SALEC_MAXMAT 10
 #define SALEC_TOLVOF 1.0e-6
@@ -183,7 +185,7 @@ __device__ __forceinline__ double second_inv(double xx, double xy, double yy, do
 }
 
 // Interval search of geometry/linear.c:196-218: leftmost/rightmost interval outside the range.
-__device__ __forceinline__ int bisearch(double x, const double *xs, int n)
+__host__ __device__ __forceinline__ int bisearch(double x, const double *xs, int n)
 {
     int lo = 0, hi = n - 1;
     if (x < xs[lo]) return lo;
@@ -201,7 +203,7 @@ __device__ __forceinline__ int bisearch(double x, const double *xs, int n)
 // both, so the index is the bisection's whatever the rounding of the bucket number. Below,
 // above and NaN take the bisection's own exits (0, n-2, n-2). Typically two dependent loads
 // instead of log2(n).
-__device__ __forceinline__ int axis_search(double x, const double *xs, int n, const int *bkt, int nb, double b0,
+__host__ __device__ __forceinline__ int axis_search(double x, const double *xs, int n, const int *bkt, int nb, double b0,
                                            double binv)
 {
     if (!bkt) return bisearch(x, xs, n);
@@ -213,6 +215,29 @@ __device__ __forceinline__ int axis_search(double x, const double *xs, int n, co
     while (g < n - 2 && xs[g + 1] <= x) ++g;
     while (g > 0 && xs[g] > x) --g;
     return g;
+}
+
+// Bucket guesses for axis_search over xs[0..n-1]: 2n uniform buckets over [xs[0], xs[n-1]);
+// bucket b holds the largest k <= n-2 with xs[k] <= xs[0] + b * width. No table (false) for an
+// axis that is not non-decreasing and finite: the device then bisects.
+inline bool build_axis_buckets(const double *xs, int n, std::vector<int> &bkt, double &b0, double &binv)
+{
+    if (n < 3) return false;
+    for (int k = 0; k < n; ++k)
+        if (!std::isfinite(xs[k]) || (k && !(xs[k] >= xs[k - 1]))) return false;
+    const double span = xs[n - 1] - xs[0];
+    const int nb = 2 * n;
+    if (!(span > 0.0) || !std::isfinite(nb / span)) return false;
+    b0 = xs[0];
+    binv = nb / span;
+    bkt.resize(nb);
+    int k = 0;
+    for (int b = 0; b < nb; ++b) {
+        const double edge = xs[0] + b * (span / nb);
+        while (k < n - 2 && xs[k + 1] <= edge) ++k;
+        bkt[b] = k;
+    }
+    return true;
 }
 
 // ------------------------------------------------------------------ Tillotson EOS

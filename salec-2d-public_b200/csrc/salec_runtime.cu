@@ -244,29 +244,6 @@ int flush_uploads(salec_gpu *h)
     return SALEC_OK;
 }
 
-// Bucket guesses for axis_search over xs[0..n-1]: 2n uniform buckets over [xs[0], xs[n-1]);
-// bucket b holds the largest k <= n-2 with xs[k] <= xs[0] + b * width. No table (false) for an
-// axis that is not non-decreasing and finite: the device then bisects.
-bool build_axis_buckets(const double *xs, int n, std::vector<int> &bkt, double &b0, double &binv)
-{
-    if (n < 3) return false;
-    for (int k = 0; k < n; ++k)
-        if (!std::isfinite(xs[k]) || (k && !(xs[k] >= xs[k - 1]))) return false;
-    const double span = xs[n - 1] - xs[0];
-    const int nb = 2 * n;
-    if (!(span > 0.0) || !std::isfinite(nb / span)) return false;
-    b0 = xs[0];
-    binv = nb / span;
-    bkt.resize(nb);
-    int k = 0;
-    for (int b = 0; b < nb; ++b) {
-        const double edge = xs[0] + b * (span / nb);
-        while (k < n - 2 && xs[k + 1] <= edge) ++k;
-        bkt[b] = k;
-    }
-    return true;
-}
-
 int upload_axis(salec_gpu *h, const double *xs, int n, const int **bkt, int *nb, double *b0, double *binv)
 {
     std::vector<int> v;
