@@ -238,23 +238,21 @@ def make_deck(n: int, folder: str) -> str:
 
 
 # ---------------------------------------------------------------- CPU reference leg
-def _cpu_reference_worker(state_path: str, n: int, steps: int, warmup: int, barrier, results) -> None:
+def _cpu_reference_worker(deck: str, eos_dir: str, steps: int, warmup: int, barrier, results) -> None:
     """One reference process of cpu_reference_cores: its own oracle instance (the reference
-    keeps global state), its own copy of the sample, timed between a common barrier and its
-    own end."""
+    keeps global state), started by the reference's own initialisation of the deck
+    (src/salec2d.c:45-105: deck, EOS tables, geometry, hydrostatic target profile, materials),
+    then timed between a common barrier and its own end. Nothing of this library runs here."""
     from oracle import ref
-    folder = tempfile.mkdtemp(prefix="salec_cpu_")
-    st = np.load(state_path)
-    deck = make_deck(n, folder)
-    ref.init(deck, folder, os.path.join(folder, "run"), material=False)
-    for name in fields.STEP_FIELDS:
-        ref.set(name, st[name])
-    ref.init_adopt(float(st["damp_time"]))
+    run_dir = tempfile.mkdtemp(prefix="salec_cpu_run_")
+    t0 = time.perf_counter()
+    ref.init(deck, eos_dir, run_dir)
+    init_s = time.perf_counter() - t0
     ref.step(warmup)
     barrier.wait()
     t0 = time.perf_counter()
     ref.step(steps)
-    results.put(time.perf_counter() - t0)
+    results.put((time.perf_counter() - t0, init_s))
 
 
 def host_cores() -> int:
@@ -268,29 +266,30 @@ def cpu_reference_cores(n: int, steps: int, warmup: int, folder: str, procs: int
     """The reference on every host core: the reference is an MPI code, single-threaded per rank,
     and the one-rank shim cannot split a domain, so each core runs its own reference process on
     its own n x n copy of the workload (the throughput an MPI run of procs ranks could reach at
-    best, with no halo exchange). All start from the library's deck-initialised state (bit-equal
-    to the reference's own init), step `warmup` cycles, meet at a barrier and step `steps`
-    cycles; the rate is procs x n^2 x steps over the slowest process's time."""
+    best, with no halo exchange). Each process starts from the reference's own initialisation of
+    the same deck, steps `warmup` cycles, meets the others at a barrier and steps `steps` cycles;
+    the rate is procs x n^2 x steps over the slowest process's time. Returns the rate, the
+    slowest timed window and the slowest initialisation."""
     import multiprocessing as mp
     deck = make_deck(n, folder)
-    sim = capi.Simulation.from_deck(deck, folder)
-    state = {name: sim.get_field(name) for name in fields.STEP_FIELDS}
-    state["damp_time"] = np.array(sim.get_run().damp_time)
-    sim.close()
-    path = os.path.join(folder, "cpu_state.npz")
-    np.savez(path, **state)
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(procs)
     results = ctx.Queue()
-    workers = [ctx.Process(target=_cpu_reference_worker, args=(path, n, steps, warmup, barrier, results))
+    workers = [ctx.Process(target=_cpu_reference_worker, args=(deck, folder, steps, warmup, barrier, results))
                for _ in range(procs)]
     for w in workers:
         w.start()
-    times = [results.get(timeout=3600) for _ in workers]
+    got = [results.get(timeout=3600) for _ in workers]
     for w in workers:
         w.join()
-    secs = max(times)
-    return procs * n * n * steps / secs, secs
+    secs = max(g[0] for g in got)
+    init_s = max(g[1] for g in got)
+    return procs * n * n * steps / secs, secs, init_s
+
+
+SAMPLE_WHY = ("the reference's own start-up of the 2048x2048 deck (its hydrostatic target profile and "
+              "material placement) takes about 10 minutes and 7.3 GB per process, so each process starts "
+              "and steps its own n x n copy of the same deck")
 
 
 def run_reference_arm(args):
@@ -300,11 +299,13 @@ def run_reference_arm(args):
     n = args.cpu_n
     procs = host_cores()
     with tempfile.TemporaryDirectory() as tmp:
-        rate, secs = cpu_reference_cores(n, args.steps, args.warmup, tmp, procs)
+        rate, secs, init_s = cpu_reference_cores(n, args.steps, args.warmup, tmp, procs)
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "cell-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload(args.n), "sample": "%dx%d cells of the same deck" % (n, n),
+                       "same_config": n == args.n, "sample_why": SAMPLE_WHY.replace("n x n", "%dx%d" % (n, n)),
+                       "start": "the reference's own initialisation in every process (%.0f s)" % init_s,
                        "parallelism": "%d reference processes, one per host core, each on its own copy "
                                       "(single-threaded per rank, no halo exchange)" % procs},
             "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
@@ -349,6 +350,127 @@ class Ranks:
             self.dist.destroy_process_group()
 
 
+def snapshot(sim, torch):
+    """Pinned host copy of a simulation's state: every step field, the tracers and the scalars."""
+    st = {}
+    for name in fields.STEP_FIELDS:
+        a = sim.get_field(name)
+        buf = torch.empty(a.size, dtype=torch.float64, pin_memory=True).numpy().reshape(a.shape)
+        buf[...] = a
+        st[name] = buf
+    return {"fields": st, "tracers": sim.get_tracers(),
+            "scalars": {k: sim.scalar(k) for k in ("dt", "time", "i_step")}}
+
+
+def restore(sim, snap, perturb=None):
+    """Upload a snapshot (optionally with m_den and m_eng scaled by 1 + perturb)."""
+    for name, a in snap["fields"].items():
+        sim.set_field(name, a * (1.0 + perturb) if perturb and name in ("m_den", "m_eng") else a)
+    sim.set_tracers(snap["tracers"])
+    for k, v in snap["scalars"].items():
+        sim.set_scalar(k, v)
+
+
+def kernel_report(sim, run, n, prof_steps, step_ms):
+    """Per-kernel device times over prof_steps cycles (CUDA events around every phase on the
+    library's stream), the algorithmic bytes of each kernel on the state reached, the dominant
+    kernel's roofline and the step-level rooflines."""
+    cells = n * n
+    nmat = run.nmat
+    pml2 = run.damp_type in (1, 2)
+    sim.profile(True)
+    sim.step(prof_steps)
+    sim.sync()
+    phase_ms, phase_cnt = sim.phase_times()
+    sim.profile(False)
+    # point classes of this state, for the algorithmic bytes of each kernel
+    vof0 = sim.get_field("m_vof")[..., 0][2:-2, 2:-2]
+    sig = sim.get_field("e_sigma")[2:-2, 2:-2]
+    damping = run.damp_type != 5 and run.damp_time > sim.scalar("time")
+    lap = sim.get_field("v_laplace")
+    # geometry read through tables of distinct rows: each table counts once per launch
+    tables = {}
+    for gname in ("v_vol", "v_subvol", "v_suf", "e_grad", "e_vol"):
+        a = sim.get_field(gname)
+        rows = {a[j].tobytes() for j in range(a.shape[0])}
+        nrow = len(rows) if len(rows) <= 512 and len(rows) < a.shape[0] else a.shape[0]
+        tables["T_" + gname] = float(nrow * a.shape[1] * a.shape[2])
+    counts = {"C": cells, "V": (n + 3) * (n + 3), "Cp": (n + 4) * (n + 4),
+              "Vl": int(np.count_nonzero(np.any(lap != 0.0, axis=-1))), **tables,
+              "Cf": int(np.count_nonzero(vof0 <= 1e-6)), "Cn": int(np.count_nonzero(vof0 < 1.0 - 1e-6)),
+              "L": int(np.count_nonzero(((sig[..., 0] > 0) | (sig[..., 1] > 0)) & (vof0 < 1.0 - 1e-6)))}
+    ntr = len(sim.get_tracers())
+    kd = {p: kernel_doubles(p, counts, nmat, pml2, damping, bool(run.porosity_model), bool(run.acoustic_fluid),
+                            ntr) for p in range(16)}
+    hbm, peak_kind = load_peaks()
+    dom = max(range(16), key=lambda p: phase_ms[p])
+    dom_ms = phase_ms[dom] / max(phase_cnt[dom], 1)
+    dom_bytes = 8.0 * kd[dom]
+    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
+    kernel_bytes_step = 8.0 * sum(kd.values())
+    manifest_bytes = 8.0 * manifest_doubles(nmat, run.damp_type, bool(run.porosity_model)) * cells
+    per_kernel = {PHASE_KERNELS[p]: {"ms": round(phase_ms[p] / phase_cnt[p], 4),
+                                     "bytes": 8.0 * kd[p],
+                                     "GBps": round(8.0 * kd[p] / (phase_ms[p] / phase_cnt[p] / 1000.0) / 1e9, 1),
+                                     "frac": round(8.0 * kd[p] / (phase_ms[p] / phase_cnt[p] / 1000.0) / 1e9 / hbm, 3)}
+                  for p in range(16) if phase_cnt[p] and kd[p] > 0}
+    return {
+        "cycle": int(sim.scalar("i_step")),
+        "kernels": per_kernel,
+        "kernel_ms": {PHASE_KERNELS[p]: round(phase_ms[p] / max(phase_cnt[p], 1), 4) for p in range(16)
+                      if phase_cnt[p]},
+        "roofline": {"bound": "hbm", "kernel": PHASE_KERNELS[dom], "achieved": achieved, "peak": hbm,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": profile_traffic(PHASE_KERNELS[dom], cells), "bytes_per_launch": dom_bytes,
+                     "launch_ms": dom_ms},
+        "step_roofline": {"manifest_bytes_per_cell_update": manifest_bytes / cells,
+                          "manifest_GBps": manifest_bytes / (step_ms / 1000.0) / 1e9,
+                          "manifest_frac": manifest_bytes / (step_ms / 1000.0) / 1e9 / hbm,
+                          "kernel_bytes_per_cell_update": kernel_bytes_step / cells,
+                          "kernel_GBps": kernel_bytes_step / (step_ms / 1000.0) / 1e9,
+                          "kernel_frac": kernel_bytes_step / (step_ms / 1000.0) / 1e9 / hbm},
+        "point_classes": counts, "tracers": ntr,
+    }
+
+
+def crater_metrics(e_den: np.ndarray, e_pos: np.ndarray, rho: float, surface: float, dx: float) -> dict:
+    """Transient-crater depth and radius from the top of the dense target (density >= rho, half the
+    target's) per column: depth = the pre-impact surface minus that height in the column next to
+    the axis; radius = the centre r of the first column, going out from the axis, where that
+    height is back at the pre-impact surface (within a tenth of a cell)."""
+    top = dense_top(e_den, e_pos, rho)
+    r = e_pos[2:-2, 2:-2, 0][0]
+    depth = float(surface - top[0])
+    back = np.nonzero(np.nan_to_num(top, nan=-np.inf) >= surface - 0.1 * dx)[0]
+    radius = float(r[back[0]]) if len(back) else None
+    return {"depth_m": depth, "radius_m": radius}
+
+
+def run_profile(sim, cycles: int, chunk: int, stream, torch, rho: float, surface: float, dx: float, e_pos):
+    """Step `cycles` cycles in chunks; the device time of every chunk from CUDA events recorded
+    around it on the library's stream (the sampling between chunks is outside them), and the
+    crater depth and radius after every chunk. Returns the chunk times and the crater history."""
+    per_chunk, hist = [], []
+    for k in range(cycles // chunk):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sim.step(chunk)
+        b.record(stream)
+        b.synchronize()
+        per_chunk.append(a.elapsed_time(b))
+        cm = crater_metrics(sim.get_field("e_den"), e_pos, rho, surface, dx)
+        cm.update({"cycle": int(sim.scalar("i_step")), "time_s": sim.scalar("time")})
+        hist.append(cm)
+    return per_chunk, hist
+
+
+def transient(hist):
+    """The sample of largest depth: the transient crater (its cycle, time, depth and radius)."""
+    k = max(range(len(hist)), key=lambda q: hist[q]["depth_m"])
+    return hist[k]
+
+
 def run_gpu_arm(args):
     import torch
     world, rank, local = dist_setup()
@@ -364,27 +486,26 @@ def run_gpu_arm(args):
     init_s = time.perf_counter() - t0
     run = sim.get_run()
     nmat = run.nmat
-    phi = 3 * nmat + 10 + (nmat + 1 if run.porosity_model else 0)
-    pml2 = run.damp_type in (1, 2)
     cells = n * n
+    dx = float(decks.config2_deck(n=n).dx)
+    snap0 = snapshot(sim, torch)          # the initial state (pinned host memory)
+    e_pos = snap0["fields"]["e_pos"]
+    den0 = snap0["fields"]["e_den"]
+    rho_half = 0.5 * float(np.median(den0[den0 > 0.0]))    # half the target's density
+    surface = float(np.nanmedian(dense_top(den0, e_pos, rho_half)))
+    stream = torch.cuda.ExternalStream(sim.stream())
 
-    # keep a host copy of the initial state for the end-to-end run (pinned host buffers)
-    init_state = {}
-    for name in fields.STEP_FIELDS:
-        a = sim.get_field(name)
-        buf = torch.empty(a.size, dtype=torch.float64, pin_memory=True).numpy().reshape(a.shape)
-        buf[...] = a
-        init_state[name] = buf
-    init_tracers = sim.get_tracers()
-
+    # the timed window starts at cycle --start-cycle of the run (untimed cycles before it)
+    if args.start_cycle > 0:
+        sim.step(args.start_cycle)
     if args.block_shapes:   # shapes given (e.g. those a plain run tuned, for a profiler capture)
         shapes = {int(p): tuple(v) for p, v in json.loads(args.block_shapes).items()}
         sim.set_block_shapes(shapes)
     else:
-        shapes = sim.autotune(cycles=4)   # untimed; block shapes of the 2-D sweeps for this mesh
+        shapes = sim.autotune(cycles=4)   # untimed; block shapes of the 2-D sweeps for this state
+    snap_start = snapshot(sim, torch) if args.start_cycle > 0 else snap0
     sim.step(args.warmup)
     sim.sync()
-    stream = torch.cuda.ExternalStream(sim.stream())
     sampler = ClockSampler(local)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -407,59 +528,17 @@ def run_gpu_arm(args):
     barrier()
     ms_max = all_max(ms)
     value = world * cells * args.steps / (ms_max / 1000.0)
-
-    # per-kernel times: a separate profiled pass (CUDA events around every phase on the
-    # library's stream), right after the timed region
-    prof_steps = min(args.steps, 50)
-    sim.profile(True)
-    sim.step(prof_steps)
-    sim.sync()
-    phase_ms, phase_cnt = sim.phase_times()
-    sim.profile(False)
-
-    # point classes of this state, for the algorithmic bytes of each kernel
-    vof0 = sim.get_field("m_vof")[..., 0][2:-2, 2:-2]
-    sig = sim.get_field("e_sigma")[2:-2, 2:-2]
-    damping = run.damp_type != 5 and run.damp_time > sim.scalar("time")
-    lap = sim.get_field("v_laplace")
-    # geometry read through tables of distinct rows: each table counts once per launch
-    tables = {}
-    for gname in ("v_vol", "v_subvol", "v_suf", "e_grad", "e_vol"):
-        a = sim.get_field(gname)
-        rows = {a[j].tobytes() for j in range(a.shape[0])}
-        nrow = len(rows) if len(rows) <= 512 and len(rows) < a.shape[0] else a.shape[0]
-        tables["T_" + gname] = float(nrow * a.shape[1] * a.shape[2])
-    counts = {"C": cells, "V": (n + 3) * (n + 3), "Cp": (n + 4) * (n + 4),
-              "Vl": int(np.count_nonzero(np.any(lap != 0.0, axis=-1))), **tables,
-              "Cf": int(np.count_nonzero(vof0 <= 1e-6)), "Cn": int(np.count_nonzero(vof0 < 1.0 - 1e-6)),
-              "L": int(np.count_nonzero(((sig[..., 0] > 0) | (sig[..., 1] > 0)) & (vof0 < 1.0 - 1e-6)))}
-    ntr = len(sim.get_tracers())
-    kd = {p: kernel_doubles(p, counts, nmat, pml2, damping, bool(run.porosity_model), bool(run.acoustic_fluid),
-                            ntr) for p in range(16)}
-
-    # dominant kernel and its roofline
-    hbm, peak_kind = load_peaks()
-    dom = max(range(16), key=lambda p: phase_ms[p])
-    dom_ms = phase_ms[dom] / max(phase_cnt[dom], 1)
-    dom_bytes = 8.0 * kd[dom]
-    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
     step_ms = ms_max / args.steps
-    kernel_bytes_step = 8.0 * sum(kd.values())
-    manifest_bytes = 8.0 * manifest_doubles(nmat, run.damp_type, bool(run.porosity_model)) * cells
-    breakdown = {PHASE_KERNELS[p]: round(phase_ms[p] / max(phase_cnt[p], 1), 4) for p in range(16) if phase_cnt[p]}
-    per_kernel = {PHASE_KERNELS[p]: {"ms": round(phase_ms[p] / phase_cnt[p], 4),
-                                     "bytes": 8.0 * kd[p],
-                                     "GBps": round(8.0 * kd[p] / (phase_ms[p] / phase_cnt[p] / 1000.0) / 1e9, 1),
-                                     "frac": round(8.0 * kd[p] / (phase_ms[p] / phase_cnt[p] / 1000.0) / 1e9 / hbm, 3)}
-                  for p in range(16) if phase_cnt[p] and kd[p] > 0}
 
-    # end to end through the C ABI with host buffers: upload the initial state from pinned
-    # host memory, K steps each reading back dt, time and the surface profile, then download
-    # the output field set
-    sim.set_scalar("time", 0.0)
+    # per-kernel times: a separate profiled pass right after the timed region
+    rep = kernel_report(sim, run, n, min(args.steps, 50), step_ms)
+
+    # end to end through the C ABI with host buffers: upload the window's start state from pinned
+    # host memory, K steps each reading back dt, time and the surface profile, then download the
+    # output field set
     out_fields = fields.OUTPUT_FIELDS
-    h2d = sum(a.nbytes for a in init_state.values()) + init_tracers.nbytes
-    d2h_step = 48 + 8 * (n + 4)   # the 48-byte scalar block (dt, time, ...) and the surface profile
+    h2d = sum(a.nbytes for a in snap_start["fields"].values()) + snap_start["tracers"].nbytes
+    d2h_step = 64 + 8 * (n + 4)   # the 64-byte scalar block (dt, time, ...) and the surface profile
     d2h_out = sum(8 * np.prod(sim.shape(f)) for f in out_fields)
     out_bufs = {f: torch.empty(int(np.prod(sim.shape(f))), dtype=torch.float64, pin_memory=True).numpy()
                 .reshape(sim.shape(f)) for f in out_fields}
@@ -468,10 +547,7 @@ def run_gpu_arm(args):
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for name, a in init_state.items():
-        sim.set_field(name, a)
-    sim.set_tracers(init_tracers)
-    sim.set_scalar("dt", run.dt)
+    restore(sim, snap_start)
     t_up = time.perf_counter()
     for _ in range(args.steps):
         sim.step_report(1, prof_buf)   # the cycle, then dt, time and the surface profile
@@ -484,12 +560,37 @@ def run_gpu_arm(args):
     e2e = world * cells * args.steps / e2e_s
     nbad = sim.check()
 
-    # mixed form (FP32 storage of the relaxed fields): same deck, same warm-up and timed steps,
-    # then its state against the plain FP64 form after the same number of cycles from the start
+    # the whole configured run in the FP64 form: device time of every chunk of cycles, the crater
+    # history, and the per-kernel table of the developed state at its end
+    whole = None
+    long64 = None
+    fields_cmp = ("e_den", "e_pre", "m_eng", "m_vof", "v_vel", "e_ste", "e_dam")
+    if args.long_cycles > 0:
+        restore(sim, snap0)
+        chunks, hist64 = run_profile(sim, args.long_cycles, args.chunk, stream, torch, rho_half, surface, dx, e_pos)
+        total_ms = sum(chunks)
+        long64 = {f: sim.get_field(f) for f in fields_cmp}
+        late_k0 = min(len(chunks) - 1, 4000 // args.chunk)
+        late = {"cycles": [late_k0 * args.chunk, (late_k0 + 1) * args.chunk],
+                "ms_per_cycle": chunks[late_k0] / args.chunk,
+                "value": cells / (chunks[late_k0] / args.chunk / 1000.0)}
+        dev = kernel_report(sim, run, n, 50, chunks[-1] / args.chunk)
+        whole = {"cycles": args.long_cycles, "chunk": args.chunk,
+                 "mean_ms_per_cycle": total_ms / args.long_cycles,
+                 "value": world * cells * args.long_cycles / (all_max(total_ms) / 1000.0),
+                 "ms_per_cycle_by_chunk": [round(c / args.chunk, 4) for c in chunks],
+                 "late_window": late, "developed_state": dev,
+                 "crater_fp64": {"transient": transient(hist64), "final": hist64[-1]},
+                 "nonfinite": sim.check()}
+
+    # mixed form (FP32 storage of the relaxed fields): same deck, same window, then its state
+    # against the plain FP64 form after the same number of cycles from the start
     mixed = None
     if not args.no_mixed:
         mix = capi.Simulation.from_deck(deck, tmp, precision=capi.PRECISION_MIXED)
-        mix.autotune(cycles=4)
+        if args.start_cycle > 0:
+            mix.step(args.start_cycle)
+        mshapes = mix.autotune(cycles=4)
         mix.step(args.warmup)
         mix.sync()
         mstream = torch.cuda.ExternalStream(mix.stream())
@@ -501,107 +602,95 @@ def run_gpu_arm(args):
         e1.synchronize()
         mms = all_max(e0.elapsed_time(e1))
         mvalue = world * cells * args.steps / (mms / 1000.0)
-        for name, a in init_state.items():
-            sim.set_field(name, a)
-        sim.set_tracers(init_tracers)
-        sim.set_scalar("dt", run.dt)
-        sim.set_scalar("time", 0.0)
-        sim.step(args.warmup + args.steps)
-        fields_cmp = ("e_den", "e_pre", "m_eng", "m_vof", "v_vel")
-        ref_state = {n: sim.get_field(n) for n in fields_cmp}
-        errs = {n: rel_l2(mix.get_field(n), ref_state[n]) for n in fields_cmp}
+        total = args.start_cycle + args.warmup + args.steps
+        restore(sim, snap0)
+        sim.step(total)
+        ref_state = {f: sim.get_field(f) for f in fields_cmp}
+        errs = {f: rel_l2(mix.get_field(f), ref_state[f]) for f in fields_cmp}
         # sensitivity of the FP64 form itself: the same run with m_den and m_eng perturbed by 1e-7
         # relative at the start (the size of one FP32 rounding)
-        for name, a in init_state.items():
-            sim.set_field(name, a * (1.0 + 1e-7) if name in ("m_den", "m_eng") else a)
-        sim.set_tracers(init_tracers)
-        sim.set_scalar("dt", run.dt)
-        sim.set_scalar("time", 0.0)
-        sim.step(args.warmup + args.steps)
-        sens = {n: rel_l2(sim.get_field(n), ref_state[n]) for n in fields_cmp}
-        den0 = init_state["e_den"]
-        rho_half = 0.5 * float(np.median(den0[den0 > 0.0]))    # half the target's density
-        surface = float(np.nanmedian(dense_top(den0, init_state["e_pos"], rho_half)))
-        d64 = crater_depth(ref_state["e_den"], init_state["e_pos"], rho_half, surface)
-        d32 = crater_depth(mix.get_field("e_den"), init_state["e_pos"], rho_half, surface)
+        restore(sim, snap0, perturb=1e-7)
+        sim.step(total)
+        sens = {f: rel_l2(sim.get_field(f), ref_state[f]) for f in fields_cmp}
+        c64 = crater_metrics(ref_state["e_den"], e_pos, rho_half, surface, dx)
+        c32 = crater_metrics(mix.get_field("e_den"), e_pos, rho_half, surface, dx)
         mixed = {"value": mvalue, "unit": "cell-updates/s", "ms_per_step": mms / args.steps,
                  "speedup_vs_fp64": mvalue / value,
                  "storage": "FP32 relaxed fields, FP64 m_vof/m_den/m_eng/m_pty/e_cvs/positions/volumes/face records",
                  "arithmetic": "f64",
-                 "rel_l2_vs_fp64": errs, "cycles_compared": args.warmup + args.steps,
+                 "rel_l2_vs_fp64": errs, "cycles_compared": total,
                  "fp64_sensitivity_rel_l2": sens,
-                 "crater_depth_m": {"fp64": d64, "mixed": d32,
-                                    "rel_err": abs(d32 - d64) / d64 if d64 > 0 else None,
-                                    "measure": "surface minus the top of density >= %.0f kg/m3 on the axis" % rho_half},
+                 "crater": {"fp64": c64, "mixed": c32,
+                            "measure": "top of density >= %.0f kg/m3 per column against the pre-impact surface"
+                                       % rho_half},
                  "nonfinite": mix.check()}
-        # the configured run length: both forms from the start to --long-cycles (untimed), then
-        # field errors and the transient crater depth of each
-        total = args.warmup + args.steps
-        if args.long_cycles > total:
-            mix.step(args.long_cycles - total)
-            for name, a in init_state.items():
-                sim.set_field(name, a)
-            sim.set_tracers(init_tracers)
-            sim.set_scalar("dt", run.dt)
-            sim.set_scalar("time", 0.0)
-            sim.step(args.long_cycles)
-            l64 = crater_depth(sim.get_field("e_den"), init_state["e_pos"], rho_half, surface)
-            l32 = crater_depth(mix.get_field("e_den"), init_state["e_pos"], rho_half, surface)
-            long64 = {n: sim.get_field(n) for n in fields_cmp}
-            long_t, bad = sim.scalar("time"), mix.check() + sim.check()
-            long_mix = {n: rel_l2(mix.get_field(n), long64[n]) for n in fields_cmp}
-            # the FP64 form's own sensitivity over the same run: m_den, m_eng perturbed by 1e-7
-            for name, a in init_state.items():
-                sim.set_field(name, a * (1.0 + 1e-7) if name in ("m_den", "m_eng") else a)
-            sim.set_tracers(init_tracers)
-            sim.set_scalar("dt", run.dt)
-            sim.set_scalar("time", 0.0)
-            sim.step(args.long_cycles)
-            lp = crater_depth(sim.get_field("e_den"), init_state["e_pos"], rho_half, surface)
+        # the configured run length: the mixed form from its window to --long-cycles with the same
+        # chunked sampling, against the FP64 whole run above
+        if long64 is not None and args.long_cycles > total:
+            mix.close()
+            mix = capi.Simulation.from_deck(deck, tmp, precision=capi.PRECISION_MIXED)
+            mix.set_block_shapes(mshapes)
+            mstream = torch.cuda.ExternalStream(mix.stream())
+            mchunks, hist32 = run_profile(mix, args.long_cycles, args.chunk, mstream, torch, rho_half, surface, dx,
+                                          e_pos)
+            long_mix = {f: rel_l2(mix.get_field(f), long64[f]) for f in fields_cmp}
+            restore(sim, snap0, perturb=1e-7)
+            pchunks, histp = run_profile(sim, args.long_cycles, args.chunk, stream, torch, rho_half, surface, dx,
+                                         e_pos)
+            t64, t32, tp = transient(hist64), transient(hist32), transient(histp)
+
+            def rel(a, b):
+                return None if a is None or b is None or b == 0 else abs(a - b) / abs(b)
+
             mixed["long_run"] = {
-                "cycles": args.long_cycles, "time_s": long_t,
+                "cycles": args.long_cycles, "time_s": hist64[-1]["time_s"],
+                "mean_ms_per_cycle": sum(mchunks) / args.long_cycles,
+                "speedup_vs_fp64_whole_run": sum(chunks) / sum(mchunks),
                 "rel_l2_vs_fp64": long_mix,
-                "fp64_sensitivity_rel_l2": {n: rel_l2(sim.get_field(n), long64[n]) for n in fields_cmp},
-                "crater_depth_m": {"fp64": l64, "mixed": l32, "fp64_perturbed": lp,
-                                   "rel_err": abs(l32 - l64) / l64 if l64 > 0 else None,
-                                   "fp64_sensitivity_rel": abs(lp - l64) / l64 if l64 > 0 else None},
-                "nonfinite": bad + sim.check()}
+                "fp64_sensitivity_rel_l2": {f: rel_l2(sim.get_field(f), long64[f]) for f in fields_cmp},
+                "transient_crater": {"fp64": t64, "mixed": t32, "fp64_perturbed": tp,
+                                     "depth_rel_err": rel(t32["depth_m"], t64["depth_m"]),
+                                     "radius_rel_err": rel(t32["radius_m"], t64["radius_m"]),
+                                     "fp64_sensitivity_depth": rel(tp["depth_m"], t64["depth_m"]),
+                                     "fp64_sensitivity_radius": rel(tp["radius_m"], t64["radius_m"])},
+                "final_crater": {"fp64": hist64[-1], "mixed": hist32[-1], "fp64_perturbed": histp[-1]},
+                "crater_history_fp64": hist64, "crater_history_mixed": hist32,
+                "nonfinite": mix.check() + sim.check()}
         mix.close()
 
     cpu = None
     if rank == 0 and not args.no_cpu:
         procs = host_cores()
         with tempfile.TemporaryDirectory() as ctmp:
-            rate, secs = cpu_reference_cores(args.cpu_n, args.cpu_steps, 2, ctmp, procs)
+            rate, secs, cinit = cpu_reference_cores(args.cpu_n, args.cpu_steps, 2, ctmp, procs)
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
                "sample": "%d steps of a %dx%d-cell copy of the workload on each of %d reference processes, "
-                         "one per host core (%.1f s)" % (args.cpu_steps, args.cpu_n, args.cpu_n, procs, secs)}
+                         "one per host core, each started by the reference's own initialisation (%.0f s); "
+                         "timed window %.1f s" % (args.cpu_steps, args.cpu_n, args.cpu_n, procs, cinit, secs)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload(n), "cells": cells, "materials": nmat, "form": "plain FP64",
+                       "window": "cycles %d-%d of the run (the timed K cycles after %d untimed cycles from the "
+                                 "deck's initial state and W warm-up cycles)"
+                                 % (args.start_cycle + args.warmup, args.start_cycle + args.warmup + args.steps,
+                                    args.start_cycle),
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "state %.1f GB, each step moves >= %.1f GB > 126 MB L2 (no flush needed)"
-                             % (h2d / 1e9, kernel_bytes_step / 1e9),
-                       "init_s": round(init_s, 2), "point_classes": counts, "tracers": ntr,
+                             % (h2d / 1e9, rep["step_roofline"]["kernel_bytes_per_cell_update"] * cells / 1e9),
+                       "init_s": round(init_s, 2), "point_classes": rep["point_classes"], "tracers": rep["tracers"],
                        "block_shapes": {PHASE_KERNELS[p]: list(v) for p, v in shapes.items()},
                        "block_shapes_by_phase": {str(p): list(v) for p, v in shapes.items()},
                        "block_shapes_source": "given" if args.block_shapes else "autotuned"},
-            "roofline": {"bound": "hbm", "kernel": PHASE_KERNELS[dom], "achieved": achieved, "peak": hbm,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": profile_traffic(PHASE_KERNELS[dom], cells), "bytes_per_launch": dom_bytes,
-                         "launch_ms": dom_ms},
-            "step_roofline": {"manifest_bytes_per_cell_update": manifest_bytes / cells,
-                              "manifest_GBps": manifest_bytes / (step_ms / 1000.0) / 1e9,
-                              "manifest_frac": manifest_bytes / (step_ms / 1000.0) / 1e9 / hbm,
-                              "kernel_bytes_per_cell_update": kernel_bytes_step / cells,
-                              "kernel_GBps": kernel_bytes_step / (step_ms / 1000.0) / 1e9,
-                              "kernel_frac": kernel_bytes_step / (step_ms / 1000.0) / 1e9 / hbm},
-            "kernels": per_kernel,
-            "kernel_ms": breakdown,
-            "e2e": {"value": e2e, "unit": "cell-updates/s", "parts": e2e_parts, "h2d_bytes_per_step": int(h2d / args.steps),
+            "roofline": rep["roofline"],
+            "step_roofline": rep["step_roofline"],
+            "kernels": rep["kernels"],
+            "kernel_ms": rep["kernel_ms"],
+            "whole_run": whole,
+            "e2e": {"value": e2e, "unit": "cell-updates/s", "parts": e2e_parts,
+                    "h2d_bytes_per_step": int(h2d / args.steps),
                     "d2h_bytes_per_step": int(d2h_step + d2h_out / args.steps)},
             "gpu_launches": launches,
             "clocks": clocks,
@@ -763,7 +852,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
     ap.add_argument("--long-cycles", type=int, default=5000,
-                    help="cycles of the mixed-vs-FP64 accuracy run at the configured length (0: skip)")
+                    help="cycles of the whole-run timing and of the mixed-vs-FP64 accuracy run at the configured "
+                         "length (0: skip)")
+    ap.add_argument("--chunk", type=int, default=250, help="cycles per timed chunk of the whole run")
+    ap.add_argument("--start-cycle", type=int, default=0,
+                    help="untimed cycles from the deck's initial state before the warm-up and timed window")
     ap.add_argument("--ensemble", type=int, default=0, help="run the ensemble mode with this many members")
     ap.add_argument("--ens-steps", type=int, default=2000)
     ap.add_argument("--ens-chunk", type=int, default=32)

@@ -243,16 +243,23 @@ int salec_boundary_map(int kind, int pattern, int nx, int ny, int ncomp, const i
  * (src/salec2d.c:167) give, for callers that cannot call cudaMalloc while they run their time
  * loop - a host code whose device memory belongs to its own pool allocator, or one that must
  * not take cudaMalloc's device-wide synchronisation inside a cycle.
- * Inputs are device planes of (nx+4) x (ny+4) doubles in the reference's cell order (x
- * fastest, two-cell pad): cell velocity r and z, sound speed, cell scales r and z (e_pos
- * components 2 and 3) and the vacuum volume fraction; dt_out is one device double; stream is
- * a cudaStream_t (NULL: the default stream); the work is enqueued, not waited for.
- * Scratch: a fixed 64 KiB array in the library's device image, held on every device that loads
- * the library until the process exits; it limits a call to 8192 * 4096 = 33554432 interior
- * cells (larger meshes return SALEC_ERR_ARG). The first call on a device looks the array up
- * with that device current and should come before any stream capture. All calls share the
- * array, so calls that overlap on the GPU race and must be ordered by the caller; each call
- * rewrites every entry it reads, so nothing needs clearing between calls.
+ * Inputs are caller-owned device planes of (nx+4) x (ny+4) doubles in the reference's cell
+ * order (x fastest, two-cell pad, row pitch exactly nx+4 with no padding between rows): cell
+ * velocity r and z, sound speed, cell scales r and z (e_pos components 2 and 3) and the vacuum
+ * volume fraction. The library's own device planes are not accepted: they have a padded pitch,
+ * and in the mixed form (SALEC_PRECISION_MIXED) the velocity and sound speed are float planes.
+ * dt_out is one device double; stream is a cudaStream_t (NULL: the default stream); the work is
+ * enqueued, not waited for.
+ * Scratch: fixed arrays in the library's device image (64 KiB of partial minima and 8 KiB of
+ * flags), held on every device that loads the library until the process exits; they limit a
+ * call to 8192 * 4096 = 33554432 interior cells (larger meshes return SALEC_ERR_ARG). Every
+ * call looks the arrays' addresses up with the caller's device current; the first call on a
+ * device also loads the library's device code there and should come before any stream capture.
+ * All calls share the arrays, so calls that overlap on the GPU race and must be ordered by the
+ * caller; each call rewrites every entry it reads, so nothing needs clearing between calls.
+ * NaN candidates follow the reference's sequential MIN (src/mpi_vec/mpi_vec_types.h:262, folded
+ * in traversal order from 1.1 * dt_prev), as salec_gpu_step does: the result is the MIN of the
+ * candidates after the last NaN, or NaN when the NaN is the last candidate.
  */
 int salec_cfl_dt_noalloc(int nx, int ny, const double *vel_r, const double *vel_z, const double *csd,
                          const double *scale_r, const double *scale_z, const double *vof_vacuum,

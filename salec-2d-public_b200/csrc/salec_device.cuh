@@ -80,6 +80,12 @@ struct Scal {
     long long i_step;
     unsigned long long nan_count; // used by salec_gpu_check
     unsigned long long aux;       // ordered-bits MAX accumulator used at initialisation
+    // NaN CFL candidates, kept as the reference's sequential MIN keeps them: the largest
+    // traversal index (j * enx + i) of a cell whose candidate is NaN (-1: none), the MIN of the
+    // candidates after it and the count of finished blocks of that recount
+    long long dt_nan_last;
+    unsigned long long dt_tail;
+    unsigned int dt_tail_blocks, pad_;
 };
 
 // Device planes of every field. R is the storage type of the "relaxed" fields: double in the

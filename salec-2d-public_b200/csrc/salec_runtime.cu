@@ -914,6 +914,8 @@ int salec_gpu_create(const salec_run_desc *run, const salec_material_desc *mats,
     s0.time = run->time;
     s0.i_step = run->i_step;
     s0.dt_acc = ord_encode(1.1 * run->dt);
+    s0.dt_nan_last = -1;
+    s0.dt_tail = ~0ULL;
     if (cudaMemcpy(h->scal, &s0, sizeof(Scal), cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(SALEC_ERR_CUDA, "scalar upload"));
 
@@ -1259,7 +1261,7 @@ int salec_gpu_set_scalar(salec_gpu *h, const char *name, double value)
     CUDA_TRY(cudaMemcpyAsync(h->scal_host, h->scal, sizeof(Scal), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     Scal s = *h->scal_host;
-    if (!strcmp(name, "dt")) { s.dt = value; s.dt_acc = ord_encode(1.1 * value); }
+    if (!strcmp(name, "dt")) { s.dt = value; s.dt_acc = ord_encode(1.1 * value); s.dt_nan_last = -1; }
     else if (!strcmp(name, "time")) s.time = value;
     else if (!strcmp(name, "i_step")) s.i_step = (long long)value;
     else return fail(SALEC_ERR_ARG, std::string("unknown scalar ") + name);

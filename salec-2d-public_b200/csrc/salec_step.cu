@@ -133,6 +133,16 @@ __device__ __forceinline__ double step_dt(const C &c)
     return dmin(c.rp.max_dt, r);
 }
 
+// CFL candidate of an interior cell that is not pure vacuum: calculate_dt (src/sale2d.c:1999-2002),
+// DTF * MIN(dt_r, dt_z) with MIN's own NaN behaviour (a NaN first argument yields the second)
+template <class C>
+__device__ __forceinline__ double cfl_candidate(const C &c, long long p, double csd)
+{
+    const double dt_r = 1.0 * PLN(c.f.e_pos, 2)[p] / (fabs(c.f.e_vel[p]) + csd);
+    const double dt_z = 1.0 * PLN(c.f.e_pos, 3)[p] / (fabs(PLN(c.f.e_vel, 1)[p]) + csd);
+    return SALEC_DTF * dmin(dt_r, dt_z);
+}
+
 // ============================================================ phase 0: surface profile
 // trace_profile (src/ejecta.c:8-63): per column, MIN of cell-centre y over cells whose vacuum
 // fraction exceeds 0.1; cells above the ejecta threshold with no vacuum get e_ejt = 1.
@@ -377,12 +387,12 @@ __global__ void SALEC_BOUNDS_GRAD k_gradient_viscosity_cfl(const CtxT<R> c)
             if (q < SALEC_TOLQPRE) q = 0.;
         }
         c.f.e_q[p] = q;
-        // CFL candidate over cells that are not pure vacuum
+        // CFL candidate over cells that are not pure vacuum; a NaN candidate is recorded by its
+        // position in the reference's traversal order instead (see k_finalize_dt)
         if (!(vof0 > 1.0 - SALEC_TOLVOF)) {
-            const double dt_r = 1.0 * PLN(c.f.e_pos, 2)[p] / (fabs(c.f.e_vel[p]) + csd);
-            const double dt_z = 1.0 * PLN(c.f.e_pos, 3)[p] / (fabs(PLN(c.f.e_vel, 1)[p]) + csd);
-            const double dt_rz = SALEC_DTF * dmin(dt_r, dt_z);
-            cand = ord_encode(dt_rz);
+            const double dt_rz = cfl_candidate(c, p, csd);
+            if (dt_rz == dt_rz) cand = ord_encode(dt_rz);
+            else atomicMax(&c.scal->dt_nan_last, (long long)j * c.d.enx + i);
         }
     }
     // block MIN, one atomic per block
@@ -400,11 +410,49 @@ __global__ void SALEC_BOUNDS_GRAD k_gradient_viscosity_cfl(const CtxT<R> c)
     }
 }
 
-// phase 6: dt of this cycle (single thread)
+// phase 6: dt of this cycle. The reference folds the candidates in traversal order (j outer, i
+// inner) with MIN(a, b) = a < b ? a : b (src/mpi_vec/mpi_vec_types.h:262), starting from
+// 1.1 * dt_prev: a NaN candidate makes the running value NaN, and the next candidate replaces
+// it. So with no NaN the result is the order-free MIN of the gradient sweep; otherwise it is
+// the MIN of the candidates after the last NaN (NaN when the NaN came last). That recount
+// runs here, over the whole grid, only when the gradient sweep saw a NaN; otherwise one thread
+// finishes the cycle's dt. The last block of a recount resets its accumulators.
+#define SALEC_FINALIZE_THREADS 256
 template <class R>
-__global__ void k_finalize_dt(const CtxT<R> c)
+__global__ void __launch_bounds__(SALEC_FINALIZE_THREADS) k_finalize_dt(const CtxT<R> c)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) c.scal->dt = step_dt(c);
+    const long long last = c.scal->dt_nan_last;
+    if (last < 0) {
+        if (threadIdx.x == 0 && blockIdx.x == 0) c.scal->dt = step_dt(c);
+        return;
+    }
+    const int nx = c.d.enx - 4;
+    const long long n = (long long)nx * (c.d.eny - 4);
+    unsigned long long best = ~0ULL;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nx) + 2, j = (int)(t / nx) + 2;
+        if ((long long)j * c.d.enx + i <= last) continue;
+        const long long p = KIDX(i, j);
+        if (c.f.m_vof[p] > 1.0 - SALEC_TOLVOF) continue;
+        best = min(best, ord_encode(cfl_candidate(c, p, (double)c.f.e_csd[p])));
+    }
+    __shared__ unsigned long long wmin[SALEC_FINALIZE_THREADS / 32];
+    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < SALEC_FINALIZE_THREADS / 32; ++w) best = min(best, wmin[w]);
+        if (best != ~0ULL) atomicMin(&c.scal->dt_tail, best);
+        __threadfence();
+        if (atomicAdd(&c.scal->dt_tail_blocks, 1u) == gridDim.x - 1) {
+            __threadfence();
+            const unsigned long long tail = atomicMin(&c.scal->dt_tail, ~0ULL);
+            const double r = tail == ~0ULL ? __longlong_as_double(0x7ff8000000000000LL) : ord_decode(tail);
+            c.scal->dt = dmin(c.rp.max_dt, r);
+            c.scal->dt_tail = ~0ULL;
+            c.scal->dt_tail_blocks = 0u;
+        }
+    }
 }
 
 // ============================================================ phase 7: vibration, stress, damage
@@ -1724,6 +1772,7 @@ __global__ void k_cycle(const CtxT<R> c)
         s->time += s->dt;
         s->i_step += 1;
         s->dt_acc = ord_encode(1.1 * s->dt);
+        s->dt_nan_last = -1;
     }
 }
 
@@ -1978,7 +2027,7 @@ void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, dim3 b, 
     case SK_CELL_VELOCITY: k_cell_velocity<R><<<g, b, 0, s>>>(c); break;
     case SK_VOID_VERTICES: k_void_vertices<R><<<gv, b, 0, s>>>(c); break;
     case SK_GRADIENT: k_gradient_viscosity_cfl<R><<<g, b, 0, s>>>(c); break;
-    case SK_FINALIZE_DT: k_finalize_dt<R><<<1, 32, 0, s>>>(c); break;
+    case SK_FINALIZE_DT: k_finalize_dt<R><<<148, SALEC_FINALIZE_THREADS, 0, s>>>(c); break;
     case SK_STRESS: SALEC_NM_DISPATCH(k_stress, c); break;
     case SK_ACCELERATION: k_vertex_acceleration<R><<<gv, b, 0, s>>>(c); break;
     case SK_DISPLACEMENT: k_vertex_displacement<R><<<gv, b, 0, s>>>(c); break;

@@ -74,6 +74,18 @@ class Material:
     epse0: float = -1.0e-5
     kappa: float = 0.98
     chi: float = 1.0
+    # Johnson-Cook keys (material.JcA ... material.JCMaxPlastic, src/sale2d_back.c:299-306); the
+    # deck carries them only when some material sets them, with the reference's defaults for
+    # the others
+    jc: Optional[Dict[str, float]] = None
+    # material.Tdelta, the shift of the melting temperature in the Ohnaka softening
+    # (src/sale2d_back.c:339); written only when some material sets it
+    tdelta: float = 0.0
+
+
+# defaults of the Johnson-Cook keys in load_state_reference (src/sale2d_back.c:299-306)
+JC_DEFAULTS = {"JcA": 4.90e7, "JcB": 1.57e8, "JcN": 1.67e-1, "JcC": 1.60e-2, "JcM": 1.70, "JcTref": 8.00e2,
+               "JcminP": -2.44e9, "JCMaxPlastic": 10.0}
 
 
 @dataclasses.dataclass
@@ -117,6 +129,11 @@ class Deck:
     temperature: str = "const"
     surf_dtdz: float = 0.0
     ejecta_threshold: float = 2.0
+    # ejecta drag (src/ejecta.c:65-133): the reference's defaults are resistance -1, friction 0
+    ejecta_resistance: float = -1.0
+    ejecta_friction: float = 0.0
+    target_temperature: float = 293.0
+    projectile_temperature: float = 293.0
     extra: Dict[str, Dict[str, str]] = dataclasses.field(default_factory=dict)
 
 
@@ -248,6 +265,45 @@ def write_sieden(path: str, name: str, nden: int = 512, neng: int = 512, seed: i
             f.write(zeros)
 
 
+def write_aneos_td(path: str, name: str, ntem: int = 120, nden: int = 160, seed: int = 11) -> None:
+    """Tabulated (temperature x density) -> (specific energy, p, c) table in the layout of
+    LoadANEOS (src/eos/eos_state.c:89-146), generated from Tillotson constants.
+
+    Layout: three comment lines, ``nTem nDen``, ``Tnorm Dnorm Pnorm``, nTem temperature nodes,
+    nTem x nDen triples (E, p, c) with the density index fastest, then nDen density nodes (the
+    reader multiplies E by the density). Temperatures span [150 K, 1.5e5 K] and densities
+    [0.05, 4] rho0, both geometrically stretched with seeded jitter of the interior nodes
+    (sorted, so strictly increasing); E = E_cold(rho) + Cv (T - 293 K), which increases with T
+    at every density, as the reader's energy bisection needs.
+    """
+    p = TILLOTSON[name]
+    rng = np.random.default_rng(seed)
+    rho0 = p["Rho0"]
+    u = np.linspace(0.0, 1.0, ntem)
+    xtem = 150.0 * (1000.0 ** u)
+    xtem[1:-1] *= 1.0 + 0.2 * (rng.random(ntem - 2) - 0.5) / ntem
+    xtem = np.sort(xtem)
+    v = np.linspace(0.0, 1.0, nden)
+    yden = 0.05 * rho0 * (80.0 ** v)
+    yden[1:-1] *= 1.0 + 0.2 * (rng.random(nden - 2) - 0.5) / nden
+    yden = np.sort(yden)
+    ec = cold_energy(p, yden)
+    T, R = np.meshgrid(xtem, yden, indexing="ij")          # [tem][den]
+    E = ec[None, :] + p["Cv"] * (T - 293.0)
+    pres, cs = tillotson_pc(p, E, R)
+    with open(path, "w") as f:
+        f.write("# synthetic ANEOS temperature-density table for %s, generated from Tillotson constants\n" % name)
+        f.write("# seed %d, %d temperatures x %d densities\n" % (seed, ntem, nden))
+        f.write("# columns: specific energy, pressure, sound speed\n")
+        f.write("%d %d\n" % (ntem, nden))
+        f.write("%.15e %.15e %.15e\n" % (293.0, rho0, 1.0e5))
+        f.write("\n".join("%.15e" % x for x in xtem) + "\n")
+        for i in range(ntem):
+            rows = np.stack([E[i], pres[i], cs[i]], axis=1)
+            f.write("\n".join("%.15e %.15e %.15e" % tuple(r) for r in rows) + "\n")
+        f.write("\n".join("%.15e" % y for y in yden) + "\n")
+
+
 def write_deck(deck: Deck, folder: str, stem: str = "deck") -> str:
     """Write ``folder/<stem>.inp`` plus one EOS file per material; return the deck path."""
     os.makedirs(folder, exist_ok=True)
@@ -259,6 +315,10 @@ def write_deck(deck: Deck, folder: str, stem: str = "deck") -> str:
             fn = os.path.join(folder, m.name + ".aneos.sd")
             if not os.path.exists(fn):
                 write_sieden(fn, m.name)
+        elif m.eos in ("aneos", "aneos.td"):
+            fn = os.path.join(folder, m.name + "." + m.eos)
+            if not os.path.exists(fn):
+                write_aneos_td(fn, m.name)
         else:
             raise ValueError("unsupported eos " + m.eos)
     radius = deck.radius_cells * deck.dy
@@ -297,7 +357,7 @@ def write_deck(deck: Deck, folder: str, stem: str = "deck") -> str:
     w("    velocity = [%s, %s]" % (_g(deck.vx), _g(deck.velocity)))
     w("    damage = [const, 0.0]")
     w("    pressure = [const, 1.0e-5]")
-    w("    temperature = [const, 293.0]")
+    w("    temperature = [const, %s]" % _g(deck.projectile_temperature))
     w("[target]")
     w("    type = plane")
     w("    number = %d" % len(deck.target_materials))
@@ -305,9 +365,9 @@ def write_deck(deck: Deck, folder: str, stem: str = "deck") -> str:
     w("    depth = %s" % _lst([_g(d) for d in deck.target_depths]))
     w("    max_depth = %s" % _g(max_depth))
     if deck.temperature == "const":
-        w("    temperature = [const, 293.0]")
+        w("    temperature = [const, %s]" % _g(deck.target_temperature))
     else:
-        w("    temperature = [conductive, 293.0]")
+        w("    temperature = [conductive, %s]" % _g(deck.target_temperature))
         w("    surf_dtdz = %s" % _g(deck.surf_dtdz))
         w("    r_planet = 1.74e6")
     w("[condition]")
@@ -350,9 +410,16 @@ def write_deck(deck: Deck, folder: str, stem: str = "deck") -> str:
     w("    epse0 = %s" % f("epse0"))
     w("    kappa = %s" % f("kappa"))
     w("    chi = %s" % f("chi"))
+    if any(m.tdelta != 0.0 for m in mats):
+        w("    Tdelta = %s" % f("tdelta"))
+    if any(m.jc for m in mats):
+        for key, dflt in JC_DEFAULTS.items():
+            w("    %s = %s" % (key, _lst([""] + [_g((m.jc or {}).get(key, dflt)) for m in mats])))
     w("[ejecta]")
     w("    threshold = %s" % _g(deck.ejecta_threshold))
-    w("    friction = 0.0")
+    if deck.ejecta_resistance != -1.0:
+        w("    resistance = %s" % _g(deck.ejecta_resistance))
+    w("    friction = %s" % ("0.0" if deck.ejecta_friction == 0.0 else _g(deck.ejecta_friction)))
     w("[numerical]")
     w("    AVISQ = %s" % _g(deck.avisq))
     w("    AVISL = %s" % _g(deck.avisl))

@@ -1,10 +1,9 @@
 """Test bridge: initialise a deck with the oracle (the reference compiled from its sources),
 hand its initialised state to the GPU library through the C ABI, and compare the two.
 
-This mirrors the reference-side integration a host driver performs:
-run-wide parameters from sale2d_var / mesh2d_info / cycle_control, per-material
-state_reference values and EOS tables, then every field's bytes as they lie in
-field_var.data.
+This mirrors the reference-side integration a host driver performs: run-wide parameters
+from sale2d_var / mesh2d_info / cycle_control, per-material state_reference values and EOS
+tables, then every field's bytes as they lie in field_var.data.
 """
 from __future__ import annotations
 
@@ -153,6 +152,43 @@ def small_deck(kind: str = "base") -> decks.Deck:
         d = decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damp_x=4, damp_y=4, damping="pml2")
         d.materials = [decks.Material("basalt_", porosity="Wunnemann", alpha0=1.0 / 0.75, alphax=1.1,
                                       epse0=-1.0e-5, kappa=0.98, chi=0.5)]
+        return d
+    if kind == "ejecta_drag":
+        # ejecta_flow (src/ejecta.c:65-133) with both the drag and the friction branch on
+        # (the threshold at half the projectile radius marks the projectile's upper cells as ejecta)
+        return decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damp_x=4, damp_y=4, velocity=-8000.0,
+                          ejecta_threshold=0.5, ejecta_resistance=40.0, ejecta_friction=0.5)
+    if kind == "aneos_td":
+        # target on a tabulated temperature-density EOS (eos_type ANEOS, src/eos/eos_state.c:793-841)
+        d = decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damp_x=4, damp_y=4, projectile="dunite_",
+                       velocity=-8000.0)
+        d.materials = [decks.Material("basalt_", eos="aneos.td"), decks.Material("dunite_")]
+        return d
+    if kind == "jc_vm":
+        # JohnsonCook1 with Collins damage, and VonMises1 (src/strength.c:470-570)
+        d = decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damp_x=4, damp_y=4, projectile="dunite_",
+                       velocity=-7000.0)
+        d.materials = [decks.Material("basalt_", yshear="JohnsonCook1", damage="Collins",
+                                      jc={"JcA": 2.0e8, "JcB": 4.0e8, "JcTref": 250.0}),
+                       decks.Material("dunite_", yshear="VonMises1", yint0=5.0e8, ydam0=1.0e8)]
+        return d
+    if kind == "jc2_vm2":
+        # JohnsonCook2 (thermal softening through the Simon melt curve) and VonMises2 with Collins
+        d = decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damp_x=4, damp_y=4, projectile="dunite_",
+                       velocity=-9000.0)
+        d.materials = [decks.Material("basalt_", yshear="JohnsonCook2",
+                                      jc={"JcA": 2.0e8, "JcB": 4.0e8, "JcTref": 250.0, "JcC": 0.05}),
+                       decks.Material("dunite_", yshear="VonMises2", damage="Collins", yint0=5.0e8, ydam0=1.0e8)]
+        return d
+    if kind == "ice":
+        # IceStrength (piecewise ice melting curve, src/strength.c:725-754); the 100 K melting shift
+        # keeps the ice below its softened melting point, so the strength is not zero
+        d = decks.Deck(npx=24, npy=32, radius_cells=4, maxstep=40, damp_x=4, damp_y=4, projectile="ice____",
+                       velocity=-6000.0)
+        d.materials = [decks.Material("ice____", poisson=0.33, yshear="IceStrength", yint0=1.0e6, yintfri=0.8,
+                                      yintlim=1.0e9, ydam0=1.0e4, ydamfri=0.6, ydamlim=1.0e9, simon_t0=273.0,
+                                      tdelta=100.0)]
+        d.target_materials = ["ice____"]
         return d
     raise KeyError(kind)
 

@@ -16,7 +16,8 @@ import pytest
 import bridge
 import trajectory as tj
 
-KINDS = ["base", "pml2_acfl", "two_mat", "sieden_projectile", "sbc_tensile", "porous", "pml3", "lubrication"]
+KINDS = ["base", "pml2_acfl", "two_mat", "sieden_projectile", "sbc_tensile", "porous", "pml3", "lubrication",
+         "ejecta_drag", "aneos_td", "jc_vm", "jc2_vm2", "ice"]
 NSTEPS = 40
 TOL_L2 = 1e-9
 TOL_DT = 1e-12
@@ -69,7 +70,8 @@ def test_step_parity(records, cuda_device, kind):
     sim.close()
 
 
-INIT_KINDS = ["base", "two_mat", "sieden_projectile", "porous", "sbc_tensile", "pml3", "lubrication"]
+INIT_KINDS = ["base", "two_mat", "sieden_projectile", "porous", "sbc_tensile", "pml3", "lubrication",
+              "ejecta_drag", "aneos_td", "jc_vm", "jc2_vm2", "ice"]
 # fields computed by the host initialiser with the reference's own arithmetic: bit-exact
 INIT_EXACT = ["v_pos", "e_pos", "e_vol", "e_grad", "v_vol", "v_subvol", "v_suf", "e_sigma", "bx_normal",
               "by_normal", "v_bf", "m_vof", "m_pty", "e_wpt", "e_tem", "e_dam"]
@@ -109,3 +111,19 @@ def test_deck_initialiser_matches_reference_init(records, cuda_device, tmp_path,
             err = tj.rel_l2(sim.get_field(n), want[n])
             assert err <= TOL_L2, "%s step %d field %s rel-L2 %.3e" % (kind, s, n, err)
     sim.close()
+
+
+@pytest.mark.gpu
+def test_ejecta_drag_branch_is_exercised(records, cuda_device):
+    """The ejecta deck's parity run only proves ejecta_flow if the drag and friction change the
+    result: the same start with both switched off must end elsewhere."""
+    rec = records["ejecta_drag"]
+    assert rec["run"]["flow_resistance"] > 0.0 and rec["run"]["flow_friction"] > 0.0
+    off = dict(rec)
+    off["run"] = dict(rec["run"], flow_resistance=-1.0, flow_friction=0.0)
+    a, b = tj.simulation_from_record(rec), tj.simulation_from_record(off)
+    a.step(10)
+    b.step(10)
+    assert tj.rel_l2(a.get_field("e_dvel"), b.get_field("e_dvel")) > 1e-6
+    a.close()
+    b.close()

@@ -118,10 +118,11 @@ def oracle_output_cases(kinds: List[str], nsteps: int, root: str) -> Dict[str, D
 CONFIG1_FIELDS = ["e_den", "e_pre", "m_eng", "m_vof", "v_vel", "e_ste", "e_dam", "y_profile"]
 
 
-def oracle_config_run(deck_fn: str, checkpoints: List[int], folder: str) -> Dict:
-    """The reference's own initialisation and time loop on a named deck (decks.<deck_fn>()),
-    recording CONFIG1_FIELDS, dt and time at each checkpoint cycle."""
-    d = getattr(bridge.decks, deck_fn)()
+def oracle_config_run(deck_fn: str, checkpoints: List[int], folder: str, deck_kwargs: Dict = None) -> Dict:
+    """The reference's own initialisation and time loop on a named deck
+    (decks.<deck_fn>(**deck_kwargs)), recording CONFIG1_FIELDS, dt and time at each checkpoint
+    cycle."""
+    d = getattr(bridge.decks, deck_fn)(**(deck_kwargs or {}))
     deck = bridge.decks.write_deck(d, folder)
     ref.init(deck, folder, os.path.join(folder, "run"))
     out = {"deck": deck, "folder": folder, "at": {}}
@@ -166,7 +167,52 @@ def oracle_noisy_deck_run_isolated(deck_kwargs: Dict, checkpoints: List[int], fo
         return ex.submit(oracle_noisy_deck_run, deck_kwargs, checkpoints, folder, seed, fields).result()
 
 
-def oracle_config_run_isolated(deck_fn: str, checkpoints: List[int], folder: str) -> Dict:
+def oracle_config_run_isolated(deck_fn: str, checkpoints: List[int], folder: str, deck_kwargs: Dict = None) -> Dict:
     ctx = mp.get_context("spawn")
     with cf.ProcessPoolExecutor(max_workers=1, mp_context=ctx) as ex:
-        return ex.submit(oracle_config_run, deck_fn, checkpoints, folder).result()
+        return ex.submit(oracle_config_run, deck_fn, checkpoints, folder, deck_kwargs).result()
+
+
+def _interior_nonvacuum_cells(m_vof: np.ndarray) -> List:
+    """Interior cells that are not pure vacuum, in the reference's traversal order of
+    calculate_dt (src/sale2d.c:1965-1978: rows j outer, columns i inner)."""
+    ny, nx = m_vof.shape[:2]
+    return [(i, j) for j in range(2, ny - 2) for i in range(2, nx - 2) if not m_vof[j, i, 0] > 1.0 - 1e-6]
+
+
+def oracle_nan_dt(kind: str, folder: str) -> Dict:
+    """The reference's own CFL phase (calculate_dt and the MIN, phases 5-6) on a mid-cycle state
+    of a small deck, with the sound speed of one cell set to NaN: the first, a middle and the
+    last cell of its traversal, and no cell. Returns the state before phase 5 (to load into the
+    GPU library) and the dt of each case."""
+    deck, folder = bridge.write_small_deck(kind, folder)
+    ref.init(deck, folder, os.path.join(folder, "run"))
+    ref.step(3)
+    ref.phases(0, 4)
+    run = bridge.run_desc_from_oracle()
+    out = {
+        "run": {n: (list(getattr(run, n)) if n == "go" else getattr(run, n)) for n in RUN_FIELDS},
+        "mats": bridge.materials_from_oracle(run.nmat),
+        "init": {n: ref.get(n) for n in bridge.UPLOAD_FIELDS},
+        "tracers0": ref.tracers(),
+        "cells": {}, "dt": {},
+    }
+    order = _interior_nonvacuum_cells(out["init"]["m_vof"])
+    dt_prev = ref.scalar("dt")
+    csd = out["init"]["e_csd"]
+    for case, cell in (("none", None), ("first", order[0]), ("middle", order[len(order) // 2]), ("last", order[-1])):
+        c = csd.copy()
+        if cell is not None:
+            c[cell[1], cell[0], 0] = np.nan
+        ref.set("e_csd", c)
+        ref.set_scalar("dt", dt_prev)
+        ref.phases(5, 6)
+        out["cells"][case] = cell
+        out["dt"][case] = ref.scalar("dt")
+    return out
+
+
+def oracle_nan_dt_isolated(kind: str, folder: str) -> Dict:
+    ctx = mp.get_context("spawn")
+    with cf.ProcessPoolExecutor(max_workers=1, mp_context=ctx) as ex:
+        return ex.submit(oracle_nan_dt, kind, folder).result()
