@@ -201,6 +201,17 @@ int salec_gpu_set_scalar(salec_gpu *h, const char *name, double value);
 int salec_gpu_set_tracers(salec_gpu *h, int n, const double *rows);
 int salec_gpu_get_tracers(salec_gpu *h, double *rows, int *n);
 
+/*
+ * Conservation sums of the current state, in FP64 with compensated (Neumaier) summation, also in
+ * the mixed form. No counterpart in the reference; the quantities are those its conservative remap
+ * and momentum update carry. out[0] total mass (sum over interior cells and materials of
+ * m_vof * e_vol * m_den), out[1] and out[2] r and z momentum (sum over active vertices of
+ * v_mass[0] * v_vel), out[3] internal energy (m_vof * e_vol * m_eng), out[4] kinetic energy
+ * (0.5 * v_mass[0] * |v_vel|^2), out[4 + m] the mass of material m = 1 .. nmat-1; n >= 4 + nmat.
+ * Synchronises the handle's stream.
+ */
+int salec_gpu_conservation(salec_gpu *h, double *out, int n);
+
 /* Count non-finite values in the evolving cell and vertex fields; SALEC_ERR_NUMERIC if any. */
 int salec_gpu_check(salec_gpu *h, long long *n_bad);
 
@@ -264,6 +275,61 @@ int salec_boundary_map(int kind, int pattern, int nx, int ny, int ncomp, const i
 int salec_cfl_dt_noalloc(int nx, int ny, const double *vel_r, const double *vel_z, const double *csd,
                          const double *scale_r, const double *scale_z, const double *vof_vacuum,
                          double dt_prev, double max_dt, double *dt_out, void *stream);
+
+/*
+ * Prescribed time steps: cycles i0 .. i0+n-1, where i0 is the handle's current cycle count, take
+ * dts[k] instead of the CFL reduction of src/sale2d.c:1959-2016 (n = 0 removes the schedule).
+ * No counterpart in the reference; it replays a recorded dt sequence, e.g. for finite-difference
+ * checks of the adjoint, which differentiates at frozen time steps.
+ */
+int salec_gpu_set_dt_schedule(salec_gpu *h, const double *dts, int n);
+
+/*
+ * Adjoint (reverse-mode derivatives) of the mesh update. No counterpart in the reference.
+ * Supported configuration: the plain FP64 form, one material beside vacuum with a Tillotson EOS,
+ * RockStrengthT yield (src/strength.c:697-722) with Ivanov or SimpleShear damage, damping = none,
+ * no porosity, acoustic fluidisation, tensile failure, tracer lubrication or ejecta drag, and
+ * partpres = 0; other handles return SALEC_ERR_UNSUPPORTED. Derivatives are those of the step at
+ * frozen time steps (the dt of each cycle as the forward run computed it); discrete quantities
+ * (void-corner counts, material flags, cut-line corner distances, the surface profile y_profile)
+ * carry none. Adjoint fields share the layout and names of the forward fields.
+ *
+ * The building blocks: salec_gpu_adjoint_reset allocates (once) and zeroes the adjoint planes and
+ * the parameter gradients; salec_gpu_adjoint_set_field / _get_field move an adjoint field in the
+ * reference's layout; salec_gpu_adjoint_phase(h, p) applies the reverse of phase p (the phases of
+ * salec_gpu_phases) with the handle's current state taken as the state before that phase: the
+ * adjoints of p's outputs become those of its inputs. salec_gpu_adjoint_params reads the
+ * accumulated d/d Yint0, Yfricint, Ydam0, Yfricdam of material 1 (RockStrengthT's cohesions and
+ * frictions, through the yield strength and the EOS pressure floor minPint/minPdam).
+ */
+int salec_gpu_adjoint_reset(salec_gpu *h);
+int salec_gpu_adjoint_set_field(salec_gpu *h, int field, const double *host, long long n);
+int salec_gpu_adjoint_get_field(salec_gpu *h, int field, double *host, long long n);
+int salec_gpu_adjoint_phase(salec_gpu *h, int phase);
+int salec_gpu_adjoint_params(salec_gpu *h, double *theta4);
+
+typedef struct salec_adjoint_result {
+    double misfit;            /* J = 0.5 * sum_i w_i (h_i - target_i)^2 at the window's end */
+    double d_params[4];       /* dJ/d Yint0, Yfricint, Ydam0, Yfricdam of material 1 */
+    double d_velocity_scale;  /* dJ/d lambda for the window's initial vertex velocities scaled by
+                                 lambda at lambda = 1 (the impactor speed U: dJ/dU = this / U) */
+} salec_adjoint_result;
+
+/*
+ * Adjoint of a window of nsteps cycles from the current state, checkpointed every `every` cycles:
+ * the window runs forward saving a checkpoint at each segment start; the misfit of the final
+ * surface-height profile is formed, h_i = sum over interior rows j of (1 - m_vof[0]) * e_pos[3]
+ * (the material column height of interior column i, a smooth stand-in for the vacuum-based
+ * y_profile), J = 0.5 * sum_i w_i (h_i - target_i)^2 with target and w (NULL: all 1) given per
+ * interior column (ncols = nx); then each segment is replayed from its checkpoint with an undo log
+ * of every phase, and the reverse phases run back to the window's start. Results: *out, the
+ * adjoint fields of the window's start (salec_gpu_adjoint_get_field) and, when grad_density is not
+ * NULL ((nx+4)*(ny+4) doubles, the cell layout), dJ/drho of every cell for a change of its initial
+ * density that scales its material densities and its cell density together. The handle is left at
+ * the window's end.
+ */
+int salec_gpu_adjoint_window(salec_gpu *h, int nsteps, int every, const double *target, const double *weight,
+                             int ncols, double *grad_density, long long n_density, salec_adjoint_result *out);
 
 /* Strength/damage/porosity function index for a reference name (case-insensitive), or -1. */
 int salec_gpu_func_index(const char *name);

@@ -54,6 +54,7 @@ struct DevMat {
     const double *cold_yeng;   // cold energy on the uniform density grid k*StepDen
     const double *xtem, *yden; // tabulated axes
     const double *data;        // [ntem][nden][3]
+    const float *data_f;       // the same table rounded to float (mixed form: FP32 interpolation)
     // bucket guesses of the axis searches (axis_search); null where an axis is not monotone
     const int *xtem_bkt, *yden_bkt;
     double xtem_b0, xtem_binv, yden_b0, yden_binv;
@@ -149,6 +150,11 @@ struct CtxT {
     const unsigned *lap_mask;
     GeoTab<R> g_v_vol, g_v_subvol, g_v_suf, g_e_grad;
     GeoTab<double> g_e_vol;
+    // prescribed time steps (null: none): cycle i_step = dt_sched_i0 + k takes dt_sched[k] for
+    // 0 <= k < dt_sched_n instead of the CFL reduction
+    const double *dt_sched;
+    long long dt_sched_i0;
+    int dt_sched_n;
 };
 using Ctx = CtxT<double>;
 
@@ -160,6 +166,15 @@ __host__ __device__ __forceinline__ double wind(double x, double lo, double hi)
     return x < lo ? lo : (x > hi ? hi : x);
 }
 __host__ __device__ __forceinline__ double sqrt_trunc(double x) { return x < 1.0e-2 ? -sqrt(fabs(x)) : sqrt(x); }
+// The same on the arithmetic type A of a sweep: double in the plain form, float where the mixed
+// form computes in FP32 (stress, strength, viscosity, stress divergence, table interpolation).
+// With A = double every operation is the FP64 form's.
+template <class A> __host__ __device__ __forceinline__ A amin(A a, A b) { return a < b ? a : b; }
+template <class A> __host__ __device__ __forceinline__ A amax(A a, A b) { return a > b ? a : b; }
+template <class A> __host__ __device__ __forceinline__ A awind(A x, A lo, A hi) { return x < lo ? lo : (x > hi ? hi : x); }
+template <class A> __host__ __device__ __forceinline__ A asqrt_trunc(A x) { return x < 1.0e-2 ? -sqrt(fabs(x)) : sqrt(x); }
+// the value of a scalar (the dual numbers of salec_dual.cuh overload it)
+__host__ __device__ __forceinline__ double val(double x) { return x; }
 
 // Order-preserving map of doubles to unsigned integers (for atomic MIN of doubles).
 __host__ __device__ __forceinline__ unsigned long long ord_encode(double v)
@@ -185,9 +200,10 @@ __host__ __device__ __forceinline__ double ord_decode(unsigned long long u)
 }
 
 // Second invariant of a (rr, rz, zz, theta) tensor: geometry/linear.c:188-194.
-__device__ __forceinline__ double second_inv(double xx, double xy, double yy, double th)
+template <class A>
+__device__ __forceinline__ A second_inv(A xx, A xy, A yy, A th)
 {
-    return ((xx - yy) * (xx - yy) + (yy - th) * (yy - th) + (th - xx) * (th - xx)) / 6.0 + xy * xy;
+    return ((xx - yy) * (xx - yy) + (yy - th) * (yy - th) + (th - xx) * (th - xx)) / A(6.0) + xy * xy;
 }
 
 // Interval search of geometry/linear.c:196-218: leftmost/rightmost interval outside the range.
@@ -248,70 +264,85 @@ inline bool build_axis_buckets(const double *xs, int n, std::vector<int> &bkt, d
 
 // ------------------------------------------------------------------ Tillotson EOS
 // Tillotson (1962) as evaluated in src/eos/eos_state.c:322-438 (TillCold, TillHot, TillTran,
-// TillPres); t = {rho0, Cv, A, B, E0, a, b, alpha, beta, Eiv, Ecv, Tref, StepDen}.
-__host__ __device__ __forceinline__ void till_pressure(const double *t, double E, double rho, double &pres, double &cs)
+// TillPres); t = {rho0, Cv, A, B, E0, a, b, alpha, beta, Eiv, Ecv, Tref, StepDen}. T is double in
+// the step and a dual number in the adjoint (its local derivatives).
+template <class T>
+__host__ __device__ __forceinline__ void till_pressure(const double *t, T E, T rho, T &pres, T &cs)
 {
     const double rho0 = t[0], A = t[2], B = t[3], E0 = t[4], a = t[5], b = t[6];
     const double al = t[7], be = t[8], Eiv = t[9], Ecv = t[10];
-    const double eta = rho / rho0;
-    const double mu = eta - 1.0;
-    const double phi0 = E / (E0 * eta * eta);
-    const double phi1 = 1.0 / (phi0 + 1.0);
+    const T eta = rho / rho0;
+    const T mu = eta - 1.0;
+    const T phi0 = E / (E0 * eta * eta);
+    const T phi1 = 1.0 / (phi0 + 1.0);
     if ((rho >= rho0) || (E < Eiv)) {
         // compressed or cold
         double Bx = eta < 1.0 ? A : B;
         pres = (a + b * phi1) * E * rho + A * mu + Bx * mu * mu;
-        double c1 = (1.0 / rho0) * (A + 2.0 * Bx * mu) + E * (a + b * phi1 * (3.0 - 2.0 * phi1));
-        double c2 = (a + b * phi1 * phi1) * pres / rho;
-        cs = sqrt_trunc(c1 + c2);
+        T c1 = (1.0 / rho0) * (A + 2.0 * Bx * mu) + E * (a + b * phi1 * (3.0 - 2.0 * phi1));
+        T c2 = (a + b * phi1 * phi1) * pres / rho;
+        cs = asqrt_trunc(c1 + c2);
     } else {
-        const double xi = rho0 / rho - 1.0;
-        double ea = 0.0, eb = 0.0;
+        const T xi = rho0 / rho - 1.0;
+        T ea = T(0.0), eb = T(0.0);
         if (al * xi * xi < 100.0) ea = exp(-1.0 * al * xi * xi);
         if (be * xi < 100.0) eb = exp(-1.0 * be * xi);
-        const double ph = a * rho * E + (b * E * rho * phi1 + A * mu * eb) * ea;
+        const T ph = a * rho * E + (b * E * rho * phi1 + A * mu * eb) * ea;
         if (E > Ecv) {
             // expanded and hot
             pres = ph;
-            double c1 = a * E + b * E * phi1 * (3.0 + 2.0 * al * xi / eta - 2.0 * phi1) * ea
-                      + A / rho0 * (1.0 - (xi / eta) * (be + 2.0 * al * xi)) * ea * eb;
-            double c2 = (a + b * phi1 * phi1 * ea) * pres / rho;
-            cs = sqrt_trunc(c1 + c2);
+            T c1 = a * E + b * E * phi1 * (3.0 + 2.0 * al * xi / eta - 2.0 * phi1) * ea
+                 + A / rho0 * (1.0 - (xi / eta) * (be + 2.0 * al * xi)) * ea * eb;
+            T c2 = (a + b * phi1 * phi1 * ea) * pres / rho;
+            cs = asqrt_trunc(c1 + c2);
         } else {
             // linear blend of the two branches between Eiv and Ecv
-            const double dT = Ecv - Eiv, dEr = E - Eiv, dEl = Ecv - E;
+            const double dT = Ecv - Eiv;
+            const T dEr = E - Eiv, dEl = Ecv - E;
             double Bx = eta < 1.0 ? A : B;
-            const double pc = (a + b * phi1) * E * rho + A * mu + Bx * mu * mu;
+            const T pc = (a + b * phi1) * E * rho + A * mu + Bx * mu * mu;
             pres = (dEl * pc + dEr * ph) / dT;
-            double cc1 = (1.0 / rho0) * (A + 2.0 * Bx * mu) + E * (a + b * phi1 * (3.0 - 2.0 * phi1));
-            double cc2 = (a + b * phi1 * phi1) * pres / rho;
-            double ch1 = a * E + b * E * phi1 * (3.0 + 2.0 * al * xi / eta - 2.0 * phi1) * ea
-                       + A / rho0 * (1.0 - (xi / eta) * (be + 2.0 * al * xi)) * ea * eb;
-            double ch2 = (a + b * phi1 * phi1 * ea) * pres / rho;
-            double c2c = cc1 + cc2;
-            double c2h = ch1 + ch2;
-            double s1 = (dEl * c2c + dEr * c2h) / dT;
-            double s2 = (ph - pc) / dT * pres / (rho * rho);
-            cs = sqrt_trunc(s1 + s2);
+            T cc1 = (1.0 / rho0) * (A + 2.0 * Bx * mu) + E * (a + b * phi1 * (3.0 - 2.0 * phi1));
+            T cc2 = (a + b * phi1 * phi1) * pres / rho;
+            T ch1 = a * E + b * E * phi1 * (3.0 + 2.0 * al * xi / eta - 2.0 * phi1) * ea
+                  + A / rho0 * (1.0 - (xi / eta) * (be + 2.0 * al * xi)) * ea * eb;
+            T ch2 = (a + b * phi1 * phi1 * ea) * pres / rho;
+            T c2c = cc1 + cc2;
+            T c2h = ch1 + ch2;
+            T s1 = (dEl * c2c + dEr * c2h) / dT;
+            T s2 = (ph - pc) / dT * pres / (rho * rho);
+            cs = asqrt_trunc(s1 + s2);
         }
     }
-    if (pres <= 1.0e-2) cs = sqrt_trunc(A / rho0);
+    if (pres <= 1.0e-2) cs = T(asqrt_trunc(A / rho0));
 }
 
 // Temperature from the cold-energy curve sampled at k*StepDen (src/eos/eos_state.c:519-526).
-__device__ __forceinline__ double till_temperature(const DevMat &m, double E, double rho)
+template <class T>
+__device__ __forceinline__ T till_temperature(const DevMat &m, T E, T rho)
 {
     const double *t = m.tl;
     const double step = t[12];
-    int dl = (int)(wind(floor(rho / step), 0, m.cold_n - 2));
-    double dxl = dl + 1.0 - rho / step;
-    double dxr = 1.0 - dxl;
-    double ecold = dxl * m.cold_yeng[dl] + dxr * m.cold_yeng[dl + 1];
-    return dmax((E - ecold) / t[1] + t[11], 0.0);
+    int dl = (int)(wind(floor(val(rho) / step), 0, m.cold_n - 2));
+    T dxl = dl + 1.0 - rho / step;
+    T dxr = 1.0 - dxl;
+    T ecold = dxl * m.cold_yeng[dl] + dxr * m.cold_yeng[dl + 1];
+    return amax((E - ecold) / t[1] + t[11], T(0.0));
 }
 
-// Bilinear table lookup over (density, specific energy): src/eos/aneos_sieden.c:264-290.
-__device__ __forceinline__ void sieden_state(const DevMat &m, double den, double eng, double &tem, double &pre, double &csd)
+// Table value k of a tabulated material on the arithmetic type: the FP64 table, or its float copy.
+template <class A>
+__device__ __forceinline__ A tab_at(const DevMat &m, size_t k)
+{
+    if constexpr (sizeof(A) == sizeof(float)) return m.data_f[k];
+    else return m.data[k];
+}
+
+// Bilinear table lookup over (density, specific energy): src/eos/aneos_sieden.c:264-290. The axis
+// searches and the interpolation weights are FP64 (the weights' differences cancel); the blend of
+// the table values runs on A.
+template <class A>
+__device__ __forceinline__ void sieden_state(const DevMat &m, double den, double eng, A &tem, A &pre, A &csd)
 {
     const double tden = den;
     const double teng = eng / den;
@@ -321,17 +352,22 @@ __device__ __forceinline__ void sieden_state(const DevMat &m, double den, double
     const double dxl = wind(1.0 - dxr, 0.0, 1.0);
     const double exr = (teng - m.xtem[ti]) / (m.xtem[tj] - m.xtem[ti]);
     const double exl = wind(1.0 - exr, 0., 1.0);
-    const double *a = m.data + ((size_t)ti * m.nden + di) * 3;
-    const double *b = m.data + ((size_t)ti * m.nden + dj) * 3;
-    const double *c = m.data + ((size_t)tj * m.nden + di) * 3;
-    const double *d = m.data + ((size_t)tj * m.nden + dj) * 3;
-    tem = (a[0] * dxl + b[0] * dxr) * exl + (c[0] * dxl + d[0] * dxr) * exr;
-    pre = (a[1] * dxl + b[1] * dxr) * exl + (c[1] * dxl + d[1] * dxr) * exr;
-    csd = (a[2] * dxl + b[2] * dxr) * exl + (c[2] * dxl + d[2] * dxr) * exr;
+    const A wr = A(dxr), wl = A(dxl), er = A(exr), el = A(exl);
+    const size_t a = ((size_t)ti * m.nden + di) * 3;
+    const size_t b = ((size_t)ti * m.nden + dj) * 3;
+    const size_t c = ((size_t)tj * m.nden + di) * 3;
+    const size_t d = ((size_t)tj * m.nden + dj) * 3;
+    tem = (tab_at<A>(m, a) * wl + tab_at<A>(m, b) * wr) * el + (tab_at<A>(m, c) * wl + tab_at<A>(m, d) * wr) * er;
+    pre = (tab_at<A>(m, a + 1) * wl + tab_at<A>(m, b + 1) * wr) * el +
+          (tab_at<A>(m, c + 1) * wl + tab_at<A>(m, d + 1) * wr) * er;
+    csd = (tab_at<A>(m, a + 2) * wl + tab_at<A>(m, b + 2) * wr) * el +
+          (tab_at<A>(m, c + 2) * wl + tab_at<A>(m, d + 2) * wr) * er;
 }
 
 // Temperature-density table with energy rows searched per density: src/eos/eos_state.c:793-841.
-__device__ __forceinline__ void aneos_td_state(const DevMat &m, double den, double eng, double &tem, double &pre, double &csd)
+// The searches and weights are FP64; the blend of pressure and sound speed runs on A.
+template <class A>
+__device__ __forceinline__ void aneos_td_state(const DevMat &m, double den, double eng, A &tem, A &pre, A &csd)
 {
     // on a monotone axis the bracketing loop of eos_state.c ends where axis_search does: 0 below
     // the axis, n-2 above it and for NaN, else the k with yden[k] <= den < yden[k+1]
@@ -349,6 +385,7 @@ __device__ __forceinline__ void aneos_td_state(const DevMat &m, double den, doub
     dxr = wind(dxr, 0.0, 1.0);
     const double dxl = 1.0 - dxr;
     auto D = [&](int it, int id, int c) { return m.data[((size_t)it * m.nden + id) * 3 + c]; };
+    auto DA = [&](int it, int id, int c) { return tab_at<A>(m, ((size_t)it * m.nden + id) * 3 + c); };
     int ti = 0, tj = m.ntem - 1;
     double ire = D(ti, di, 0) * dxl + D(ti, dj, 0) * dxr;
     double jre = D(tj, di, 0) * dxl + D(tj, dj, 0) * dxr;
@@ -360,171 +397,274 @@ __device__ __forceinline__ void aneos_td_state(const DevMat &m, double den, doub
     double txr = (eng - ire) / (jre - ire);
     txr = wind(txr, 0.0, 1.0);
     const double txl = 1.0 - txr;
-    tem = m.xtem[ti] * txl + m.xtem[tj] * txr;
-    pre = (D(ti, di, 1) * dxl + D(ti, dj, 1) * dxr) * txl + (D(tj, di, 1) * dxl + D(tj, dj, 1) * dxr) * txr;
-    csd = (D(ti, di, 2) * dxl + D(ti, dj, 2) * dxr) * txl + (D(tj, di, 2) * dxl + D(tj, dj, 2) * dxr) * txr;
+    tem = A(m.xtem[ti] * txl + m.xtem[tj] * txr);
+    const A wl = A(dxl), wr = A(dxr), ul = A(txl), ur = A(txr);
+    pre = (DA(ti, di, 1) * wl + DA(ti, dj, 1) * wr) * ul + (DA(tj, di, 1) * wl + DA(tj, dj, 1) * wr) * ur;
+    csd = (DA(ti, di, 2) * wl + DA(ti, dj, 2) * wr) * ul + (DA(tj, di, 2) * wl + DA(tj, dj, 2) * wr) * ur;
 }
 
 // calculate_state_correct with CAP_MINPRESSURE (src/eos/eos_state.c:747-791): porosity-scaled
-// state, porous sound speed, pressure floor.
+// state, porous sound speed, pressure floor. The Tillotson form is evaluated in FP64 (its
+// compression mu = rho/rho0 - 1 cancels); the tabulated forms interpolate on A.
+template <class A>
 __device__ __forceinline__ void material_state(const DevMat &m, double den, double eng, double plim, double pty,
-                                               double &tem, double &pre, double &csd)
+                                               A &tem, A &pre, A &csd)
 {
-    double t = 0., p = 0., c = 0.;
+    A t = A(0.), p = A(0.), c = A(0.);
     const double d = den * pty, e = eng * pty;
     if (m.eos_type == 1) {
         const double ein = e / d;
-        t = till_temperature(m, ein, d);
-        till_pressure(m.tl, ein, d, p, c);
+        double pd, cd;
+        t = A(till_temperature(m, ein, d));
+        till_pressure(m.tl, ein, d, pd, cd);
+        p = A(pd);
+        c = A(cd);
     } else if (m.eos_type == 2) {
-        sieden_state(m, d, e, t, p, c);
+        sieden_state<A>(m, d, e, t, p, c);
     } else {
-        aneos_td_state(m, d, e, t, p, c);
+        aneos_td_state<A>(m, d, e, t, p, c);
     }
-    p = p / pty;
-    if (pty > 1.0) c *= (1.0 + (m.chi - 1.0) * fmax(0.0, fmin(1.0, (pty - 1.0) / (m.alpha0 - 1.0))));
-    if (p < plim) p = dmax(p, plim);
+    p = p / A(pty);
+    if (pty > 1.0) c *= A(1.0 + (m.chi - 1.0) * fmax(0.0, fmin(1.0, (pty - 1.0) / (m.alpha0 - 1.0))));
+    if (p < A(plim)) p = amax(p, A(plim));
     tem = t; pre = p; csd = c;
 }
 
+// ------------------------------------------------------------------ flux geometry
+// Pieces of calculate_flux_mixed (src/advect.c:861-1136), templates on the scalar type (double
+// in the step, a dual number in the adjoint).
+template <class T>
+__device__ __forceinline__ T swept_volume(double xa, double ya, double xb, double yb, T dxa, T dya, T dxb, T dyb)
+{
+    // get_flux_volcyl (src/advect.c:1347-1354)
+    const T x1 = -1.0 * dxa, y1 = -1.0 * dya, x2 = -1.0 * dxb, y2 = -1.0 * dyb;
+    const T vol = x1 * (ya - yb - y2) + x2 * (ya - yb + y1) + (y1 + y2) * (xb - xa);
+    return vol * fabs(2.0 * xa + 2.0 * xb + x1 + x2) / 8.0;
+}
+
+template <class T>
+__device__ __forceinline__ T face_ratio(T p1, T p2)
+{
+    // geometric_flux_ratio (src/advect.c:1312-1330)
+    T a = p1, b = p2;
+    if (b > a) { a = p2; b = p1; }
+    if (b >= 0.0) return T(1.0);
+    if (a <= 0.0) return T(0.0);
+    return a / (a + fabs(b));
+}
+
+template <class T>
+__device__ __forceinline__ T cut_length(T vf, T a, T b)
+{
+    // cut_length / cut_length_l / cut_length_s (src/advect.c:1356-1407)
+    if (a < b) { T t = a; a = b; b = t; }
+    if (1.0e-5 * a > b) {
+        T d;
+        if (vf <= 0.0) d = T(0.0);
+        else if (vf <= 1.0) d = vf * a;
+        else d = a;
+        return d + b;
+    }
+    const T crf1 = 0.5 * b / a;
+    if (vf <= crf1) return sqrt(2.0 * a * b * vf);
+    if (vf <= 1.0 - crf1) return 0.5 * b + a * vf;
+    if (vf <= 1.0) return a + b - sqrt(2.0 * a * b * (1.0 - vf));
+    return a + b;
+}
+
+template <class T>
+__device__ __forceinline__ void normalise2(T &x, T &y)
+{
+    // vec_norm (src/geometry/linear.c:132-146)
+    T len = T(0.);
+    len += x * x;
+    len += y * y;
+    len = sqrt(len);
+    x /= len;
+    if (isnan(val(x))) x = T(1.0);
+    y /= len;
+    if (isnan(val(y))) y = T(1.0);
+}
+
+__device__ __forceinline__ double mstacs(double nd, double gf, double cr)
+{
+    // vofMSTACS (src/advect.c:1259-1274)
+    double cds, st;
+    if (cr < 1.0 / 3.0) cds = dmin(nd / cr, 1.0);
+    else cds = dmin(3.0 * nd, 1.0);
+    if (nd < 1.0 / 5.0) st = 3.0 * nd;
+    else if (nd < 1.0 / 2.0) st = (1.0 + nd) / 2.0;
+    else st = dmin((6.0 * nd + 3.0) / 8.0, 1.0);
+    return gf * cds + (1.0 - gf) * st;
+}
+
+__device__ __forceinline__ double algebraic_ratio(double vu, double vd, double va, double cr, double nx, double ny,
+                                                  double gx, double gy)
+{
+    // algebraic_flux_ratio (src/advect.c:1226-1253)
+    const double tmp = va - vu;
+    const double nd = (vd - vu) / tmp;
+    if (fabs(tmp) < SALEC_TOLVOF) return vd;
+    if (nd < SALEC_TOLVOF || nd > 1.0 - SALEC_TOLVOF) return vd;
+    double dot = 0.; dot += gx * nx; dot += gy * ny;
+    double len = 0.; len += gx * gx; len += gy * gy;
+    double cost = dot / sqrt(len);
+    cost = cost * cost;
+    const double gf = dmin(SALEC_CISSAMK1 * cost * cost, 1.0);
+    return vu + mstacs(nd, gf, cr) * (va - vu);
+}
+
 // ------------------------------------------------------------------ strength model pieces
-// Published forms as written in src/strength.c:505-570.
-__device__ __forceinline__ double y_lundborg(double p, double y0, double fric, double ylim)
+// Published forms as written in src/strength.c:505-570, on the arithmetic type A.
+template <class A>
+__device__ __forceinline__ A y_lundborg(A p, A y0, A fric, A ylim)
 {
-    return y0 + p * fric / (1 + p * fric / (ylim - y0));
+    return y0 + p * fric / (A(1) + p * fric / (ylim - y0));
 }
-__device__ __forceinline__ double y_drucker(double p, double y0, double fric, double ylim)
+template <class A>
+__device__ __forceinline__ A y_drucker(A p, A y0, A fric, A ylim)
 {
-    return dmin(y0 + fric * p, ylim);
+    return amin(y0 + fric * p, ylim);
 }
-__device__ __forceinline__ double simon_melt(double pre, const DevMat &s)
+template <class A>
+__device__ __forceinline__ A simon_melt(A pre, const DevMat &s)
 {
-    double sol = s.Tmelt0 * pow(s.Asimon * pre + 1.0, s.Csimon);
+    A sol = A(s.Tmelt0) * pow(A(s.Asimon) * pre + A(1.0), A(s.Csimon));
     if (s.PolyLiq <= 0 && s.PolySol <= 0) return sol;
     if (s.PolySol > 0) {
-        double pg = pre * 1.0e-9;
-        sol = s.Tsolc1 + s.Tsolc2 * pg + s.Tsolc3 * pg * pg;
+        A pg = pre * A(1.0e-9);
+        sol = A(s.Tsolc1) + A(s.Tsolc2) * pg + A(s.Tsolc3) * pg * pg;
     }
-    double pg = pre * 1.0e-9;
-    double liq = s.Tlidc1 + s.Tlidc2 * pg + s.Tlidc3 * pg * pg;
-    return dmax(sol, liq);
+    A pg = pre * A(1.0e-9);
+    A liq = A(s.Tlidc1) + A(s.Tlidc2) * pg + A(s.Tlidc3) * pg * pg;
+    return amax(sol, liq);
 }
-__device__ __forceinline__ double ohnaka_soft(double tem, const DevMat &s, double tmelt)
+template <class A>
+__device__ __forceinline__ A ohnaka_soft(A tem, const DevMat &s, A tmelt)
 {
-    return tanh(((tmelt + s.Tdelta) / tem - 1.0) * s.Tfrac);
+    return tanh(((tmelt + A(s.Tdelta)) / tem - A(1.0)) * A(s.Tfrac));
 }
-__device__ __forceinline__ double jnck_soft(double tem, double pre, const DevMat &s)
+template <class A>
+__device__ __forceinline__ A jnck_soft(A tem, A pre, const DevMat &s)
 {
-    double tm = simon_melt(pre, s);
-    double mf = (tem - s.JCTREF) / (tm - s.JCTREF);
-    mf = wind(mf, 0.0, 1.0);
-    return wind(1.0 - pow(mf, s.JCM), 0.0, 1.0);
+    A tm = simon_melt<A>(pre, s);
+    A mf = (tem - A(s.JCTREF)) / (tm - A(s.JCTREF));
+    mf = awind(mf, A(0.0), A(1.0));
+    return awind(A(1.0) - pow(mf, A(s.JCM)), A(0.0), A(1.0));
 }
-__device__ __forceinline__ double ice_melt(double p)
+template <class A>
+__device__ __forceinline__ A ice_melt(A p)
 {
     // piecewise ice melting curve with a Simon-type high-pressure branch (src/strength.c:725-754)
-    const double p0 = 0.0, p1 = 0.2e9, p2 = 0.34e9, p3 = 0.61e9, p4 = 2.17e9;
-    const double t0 = 273.0, t1 = 252.0, t2 = 257.0, t3 = 274.0, t4 = 354.8;
+    const A p0 = A(0.0), p1 = A(0.2e9), p2 = A(0.34e9), p3 = A(0.61e9), p4 = A(2.17e9);
+    const A t0 = A(273.0), t1 = A(252.0), t2 = A(257.0), t3 = A(274.0), t4 = A(354.8);
     if (p <= p1) return t0 + (t1 - t0) * (p - p0) / (p1 - p0);
     else if (p > p1 && p <= p2) return t1 + (t2 - t1) * (p - p1) / (p2 - p1);
     else if (p > p2 && p <= p3) return t2 + (t3 - t2) * (p - p2) / (p3 - p2);
     else if (p > p3 && p <= p4) return t3 + (t4 - t3) * (p - p3) / (p4 - p3);
-    return t4 * pow(((p - p4) / 1.253e9) + 1, 1.0 / 3.0);
+    return t4 * pow(((p - p4) / A(1.253e9)) + A(1), A(1.0 / 3.0));
 }
 
-// The registry of src/strength.c:860-875 as one dispatcher. pa = {pressure, damage, plastic
-// strain, strain rate, temperature, ...} (porosity uses its own six arguments); passed by value
-// so that no caller keeps an array in local memory.
-static __device__ __noinline__ double strength_fn(int id, double p0, double p1, double p2, double p3, double p4,
-                                                  double p5, const DevMat &s)
+// RockStrengthT (src/strength.c:697-722) with its cohesions, frictions and limits as arguments, so
+// that the adjoint can differentiate with respect to them.
+template <class A>
+__device__ __forceinline__ A rock_strength_t(A pre, A dam, A dps, A temp, A yint0, A fint, A ylimint, A ydam0, A fdam,
+                                             A ylimdam, const DevMat &s)
 {
-    const double pa[6] = {p0, p1, p2, p3, p4, p5};
-    const double BETA = 0.57735026918962576451;   // JohnsonCook factor as in interpolate_fn.h
+    A yint = y_lundborg<A>(pre, yint0, fint, ylimint);
+    A ydam = y_drucker<A>(pre, ydam0, fdam, ylimdam);
+    ydam = amin(yint, ydam);
+    A tm = simon_melt<A>(pre, s);
+    A soft = ohnaka_soft<A>(temp, s, tm);
+    soft = awind(soft, A(0.0), A(1.0));
+    A ymed = (ydam * dam + yint * (A(1.0) - dam)) * soft;
+    A yvis = dps * A(s.melt_viscosity) * (A(1.0) - soft);
+    return amax(ymed, yvis);
+}
+
+// The registry of src/strength.c:860-875 as one dispatcher, on the arithmetic type A. pa =
+// {pressure, damage, plastic strain, strain rate, temperature, ...} (porosity uses its own six
+// arguments); passed by value so that no caller keeps an array in local memory.
+template <class A>
+static __device__ __noinline__ A strength_fn(int id, A p0, A p1, A p2, A p3, A p4, A p5, const DevMat &s)
+{
+    const A pa[6] = {p0, p1, p2, p3, p4, p5};
+    const A BETA = A(0.57735026918962576451);   // JohnsonCook factor as in interpolate_fn.h
     switch (id) {
     case 0: { // SimpleRock (never selectable in the reference: str2func rejects index 0)
-        double yint = y_lundborg(pa[0], s.Yint0, s.Yfricint, s.Ylimint);
-        double ydam = y_drucker(pa[0], s.Ydam0, s.Yfricdam, s.Ylimdam);
-        ydam = dmin(yint, ydam);
-        return ydam * pa[1] + yint * (1.0 - pa[1]);
+        A yint = y_lundborg<A>(pa[0], A(s.Yint0), A(s.Yfricint), A(s.Ylimint));
+        A ydam = y_drucker<A>(pa[0], A(s.Ydam0), A(s.Yfricdam), A(s.Ylimdam));
+        ydam = amin(yint, ydam);
+        return ydam * pa[1] + yint * (A(1.0) - pa[1]);
     }
     case 1: case 7: // SimpleShear / Ivanov damage increment
-        return 1.0 / dmax(s.IvanA, s.IvanB * (pa[0] - s.IvanC));
+        return A(1.0) / amax(A(s.IvanA), A(s.IvanB) * (pa[0] - A(s.IvanC)));
     case 2: case 3: { // JohnsonCook1 / JohnsonCook2
-        double ps = wind(pa[2], 0.0, s.JCMaxPlastic);
-        double y1 = s.JCA + s.JCB * pow(ps, s.JCN);
-        double y2 = 1.0;
-        if (pa[3] > 1.0 && s.JCC > 0.0) y2 = 1.0 + s.JCC * log(pa[3]);
-        if (id == 3) return y1 * y2 * jnck_soft(pa[4], pa[0], s) * BETA;
+        A ps = awind(pa[2], A(0.0), A(s.JCMaxPlastic));
+        A y1 = A(s.JCA) + A(s.JCB) * pow(ps, A(s.JCN));
+        A y2 = A(1.0);
+        if (pa[3] > A(1.0) && s.JCC > 0.0) y2 = A(1.0) + A(s.JCC) * log(pa[3]);
+        if (id == 3) return y1 * y2 * jnck_soft<A>(pa[4], pa[0], s) * BETA;
         return y1 * y2 * BETA;
     }
-    case 4: { // RockStrengthT
-        double pre = pa[0], dam = pa[1];
-        double dps = pa[3], temp = pa[4];
-        double yint = y_lundborg(pre, s.Yint0, s.Yfricint, s.Ylimint);
-        double ydam = y_drucker(pre, s.Ydam0, s.Yfricdam, s.Ylimdam);
-        ydam = dmin(yint, ydam);
-        double tm = simon_melt(pre, s);
-        double soft = ohnaka_soft(temp, s, tm);
-        soft = wind(soft, 0.0, 1.0);
-        double ymed = (ydam * dam + yint * (1.0 - dam)) * soft;
-        double yvis = dps * s.melt_viscosity * (1.0 - soft);
-        return dmax(ymed, yvis);
-    }
+    case 4: // RockStrengthT
+        return rock_strength_t<A>(pa[0], pa[1], pa[3], pa[4], A(s.Yint0), A(s.Yfricint), A(s.Ylimint), A(s.Ydam0),
+                                  A(s.Yfricdam), A(s.Ylimdam), s);
     case 5: { // IceStrength
-        double pre = pa[0], dam = pa[1], temp = pa[4];
-        double yint = y_lundborg(pre, s.Yint0, s.Yfricint, s.Ylimint);
-        double ydam = y_lundborg(pre, s.Ydam0, s.Yfricdam, s.Ylimdam);
-        ydam = dmin(yint, ydam);
-        double tm = ice_melt(pre);
-        double soft = ohnaka_soft(temp, s, tm);
-        soft = wind(soft, 0.0, 1.0);
-        return (ydam * dam + yint * (1.0 - dam)) * soft;
+        A pre = pa[0], dam = pa[1], temp = pa[4];
+        A yint = y_lundborg<A>(pre, A(s.Yint0), A(s.Yfricint), A(s.Ylimint));
+        A ydam = y_lundborg<A>(pre, A(s.Ydam0), A(s.Yfricdam), A(s.Ylimdam));
+        ydam = amin(yint, ydam);
+        A tm = ice_melt<A>(pre);
+        A soft = ohnaka_soft<A>(temp, s, tm);
+        soft = awind(soft, A(0.0), A(1.0));
+        return (ydam * dam + yint * (A(1.0) - dam)) * soft;
     }
     case 6: { // Collins damage increment
-        double pre = pa[0], inc;
-        if (pre < s.Pbd) inc = dmax(0.01, 0.01 + 0.04 * pre / s.Pbd);
-        else if (pre < s.Pbp) inc = 0.05 + 0.05 * (pre - s.Pbd) / (s.Pbp - s.Pbd);
-        else inc = 0.1 + 0.5 * (pre - s.Pbp) / s.Pbp;
-        return 1.0 / inc;
+        A pre = pa[0], inc;
+        if (pre < A(s.Pbd)) inc = amax(A(0.01), A(0.01) + A(0.04) * pre / A(s.Pbd));
+        else if (pre < A(s.Pbp)) inc = A(0.05) + A(0.05) * (pre - A(s.Pbd)) / (A(s.Pbp) - A(s.Pbd));
+        else inc = A(0.1) + A(0.5) * (pre - A(s.Pbp)) / A(s.Pbp);
+        return A(1.0) / inc;
     }
     case 8: { // SimpleTensile
-        double tm = simon_melt(pa[0], s);
-        double soft = ohnaka_soft(pa[4], s, tm);
-        soft = wind(soft, 0.0, 1.0);
-        return s.Yten0 * (1.0 - pa[1]) * soft;
+        A tm = simon_melt<A>(pa[0], s);
+        A soft = ohnaka_soft<A>(pa[4], s, tm);
+        soft = awind(soft, A(0.0), A(1.0));
+        return A(s.Yten0) * (A(1.0) - pa[1]) * soft;
     }
     case 11: { // VonMises1
-        double yint = s.Yint0, ydam = dmin(yint, s.Ydam0);
-        return ydam * pa[1] + yint * (1.0 - pa[1]);
+        A yint = A(s.Yint0), ydam = amin(yint, A(s.Ydam0));
+        return ydam * pa[1] + yint * (A(1.0) - pa[1]);
     }
     case 12: { // VonMises2
-        double yint = s.Yint0, ydam = dmin(yint, s.Ydam0);
-        double tm = simon_melt(pa[0], s);
-        double soft = wind(ohnaka_soft(pa[4], s, tm), 0.0, 1.0);
-        return (ydam * pa[1] + yint * (1.0 - pa[1])) * soft;
+        A yint = A(s.Yint0), ydam = amin(yint, A(s.Ydam0));
+        A tm = simon_melt<A>(pa[0], s);
+        A soft = awind(ohnaka_soft<A>(pa[4], s, tm), A(0.0), A(1.0));
+        return (ydam * pa[1] + yint * (A(1.0) - pa[1])) * soft;
     }
     case 10: { // Wunnemann et al. (2006) epsilon-alpha porosity rate (src/strength.c:801-854)
-        double pty = pa[0], cvs = pa[1], pre = pa[2], dcvs = pa[3], evx = pa[4], evy = pa[5];
-        if (pty <= 1.0 || pty > s.alphamax || pre <= 0.) return 0.;
-        double v2 = evx * evx + evy * evy;
-        if (v2 <= s.avel * s.avel) return 0.;
-        double cvs_c;
-        if (pty > s.alphae) cvs_c = s.epse0;
-        else if (pty > s.alphax) cvs_c = s.epse0 + log(pty / s.alphae) / s.kappa;
-        else cvs_c = s.epsec - sqrt((pty - 1.0) / (s.alphax - 1.0)) * (s.epsec - s.epsex);
-        double ratio = 1.0 + (s.chi - 1.0) * fmax(0.0, fmin(1.0, (pty - 1.0) / (s.alphamax - 1.0)));
-        double dade = pty * (1.0 - ratio * ratio);
-        if (dcvs < 0. && cvs < cvs_c) {
-            if (pty > s.alphax) dade = s.kappa * pty;
-            else dade = sqrt((pty - 1.) / (s.alphax - 1.0)) * s.kappa * s.alphax;
+        A pty = pa[0], cvs = pa[1], pre = pa[2], dcvs = pa[3], evx = pa[4], evy = pa[5];
+        if (pty <= A(1.0) || pty > A(s.alphamax) || pre <= A(0.)) return A(0.);
+        A v2 = evx * evx + evy * evy;
+        if (v2 <= A(s.avel) * A(s.avel)) return A(0.);
+        A cvs_c;
+        if (pty > A(s.alphae)) cvs_c = A(s.epse0);
+        else if (pty > A(s.alphax)) cvs_c = A(s.epse0) + log(pty / A(s.alphae)) / A(s.kappa);
+        else cvs_c = A(s.epsec) - sqrt((pty - A(1.0)) / (A(s.alphax) - A(1.0))) * (A(s.epsec) - A(s.epsex));
+        A ratio = A(1.0) + (A(s.chi) - A(1.0)) * fmax(A(0.0), fmin(A(1.0), (pty - A(1.0)) / (A(s.alphamax) - A(1.0))));
+        A dade = pty * (A(1.0) - ratio * ratio);
+        if (dcvs < A(0.) && cvs < cvs_c) {
+            if (pty > A(s.alphax)) dade = A(s.kappa) * pty;
+            else dade = sqrt((pty - A(1.)) / (A(s.alphax) - A(1.0))) * A(s.kappa) * A(s.alphax);
         } else {
-            dade = pty * (1.0 - ratio * ratio);
+            dade = pty * (A(1.0) - ratio * ratio);
         }
         return dade * dcvs;
     }
     case 9:
     default:
-        return 0.0;
+        return A(0.0);
     }
 }
 

@@ -3,6 +3,7 @@
 #include "../../include/salec_gpu.h"
 #include "salec_device.cuh"
 #include "salec_kernels.h"
+#include "salec_adjoint.h"
 
 #include <cuda_runtime.h>
 
@@ -104,6 +105,7 @@ struct Gather {
     GatherBatch batch{};
     bool two_pass = false;
     int ncomp_max = 0;
+    int entries[SALEC_MAX_GATHER_FIELDS] = {0};   // map entries per field (the adjoint walks entries)
 };
 
 } // namespace
@@ -164,6 +166,12 @@ struct salec_gpu {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool fork_tracers = false;
     void *output = nullptr;     // output writer state (salec_output.cu)
+    void *conserve = nullptr;   // scratch of the conservation sums (salec_conserve.cu)
+    // prescribed time steps (salec_gpu_set_dt_schedule)
+    double *dt_sched = nullptr;
+    long long dt_sched_i0 = 0;
+    int dt_sched_n = 0;
+    struct AdjointState *adj = nullptr;   // adjoint buffers (salec_gpu_adjoint_*)
 
     template <class R>
     CtxT<R> ctx_t() const
@@ -181,6 +189,9 @@ struct salec_gpu {
         c.g_v_suf = {static_cast<const R *>(geo[2].tab), geo[2].row, geo[2].plane};
         c.g_e_grad = {static_cast<const R *>(geo[3].tab), geo[3].row, geo[3].plane};
         c.g_e_vol = {static_cast<const double *>(geo[4].tab), geo[4].row, geo[4].plane};
+        c.dt_sched = dt_sched;
+        c.dt_sched_i0 = dt_sched_i0;
+        c.dt_sched_n = dt_sched_n;
         return c;
     }
     Ctx ctx() const { return ctx_t<double>(); }
@@ -286,6 +297,7 @@ int make_gather(salec_gpu *h, Gather &g, const std::vector<std::pair<int, Gather
         if (rc) return rc;
         if (comp && (rc = upload_vec(h, cstart[k], &gf.cstart))) return rc;
         g.batch.start[k] = total;
+        g.entries[k] = (int)m.dst.size();
         total += comp ? (int)cstart[k].size() - 1 : (int)m.dst.size();
     }
     g.batch.start[maps.size()] = total;
@@ -459,6 +471,10 @@ int upload_material(salec_gpu *h, const salec_material_desc &m, DevMat &dm)
         if ((rc = upload_vec(h, x, &dm.xtem))) return rc;
         if ((rc = upload_vec(h, y, &dm.yden))) return rc;
         if ((rc = upload_vec(h, t, &dm.data))) return rc;
+        if (h->mixed) {   // the mixed form interpolates the table in FP32
+            std::vector<float> tf(t.begin(), t.end());
+            if ((rc = upload_vec(h, tf, &dm.data_f))) return rc;
+        }
         if ((rc = upload_axis(h, x.data(), m.ntem, &dm.xtem_bkt, &dm.xtem_nb, &dm.xtem_b0, &dm.xtem_binv))) return rc;
         if ((rc = upload_axis(h, y.data(), m.nden, &dm.yden_bkt, &dm.yden_nb, &dm.yden_b0, &dm.yden_binv))) return rc;
     } else {
@@ -683,10 +699,15 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
     return SALEC_OK;
 }
 
+void adjoint_release(salec_gpu *h);
+
 void release(salec_gpu *h)
 {
     if (!h) return;
     salec_internal_output_release(h->output);
+    if (h->conserve) cudaFree(h->conserve);
+    if (h->dt_sched) cudaFree(h->dt_sched);
+    adjoint_release(h);
     for (void *p : h->owned) cudaFree(p);
     if (h->pool) cudaFree(h->pool);
     if (h->staging) cudaFree(h->staging);
@@ -768,6 +789,7 @@ Tracers salec_internal_tracers(salec_gpu *h) { return h->tr; }
 Dims salec_internal_dims(salec_gpu *h) { return h->d; }
 void salec_internal_add_launches(salec_gpu *h, int n) { h->launches += n; }
 void *&salec_internal_output_slot(salec_gpu *h) { return h->output; }
+void *&salec_internal_conserve_slot(salec_gpu *h) { return h->conserve; }
 
 // ================================================================== C ABI
 extern "C" {
@@ -1374,6 +1396,473 @@ int salec_gpu_check(salec_gpu *h, long long *n_bad)
     bad = h->scal_host->nan_count;
     if (n_bad) *n_bad = (long long)bad;
     return bad ? fail(SALEC_ERR_NUMERIC, std::to_string(bad) + " non-finite values") : SALEC_OK;
+}
+
+} // extern "C"
+
+// ================================================================== adjoint of a window of cycles
+// The reverse sweeps live in salec_adjoint.cu; this part keeps their buffers, replays the forward
+// cycles with an undo log, and runs the sweeps in reverse order.
+struct AdjointState {
+    char *pool = nullptr;          // adjoint planes, laid out as the field pool
+    Fields b{};
+    double *theta = nullptr;       // d/d Yint0, Yfricint, Ydam0, Yfricdam of material 1
+    double *gscratch = nullptr;    // reverse-gather scratch
+    size_t gscratch_doubles = 0;
+    char *tmp = nullptr;           // forward fields of a phase kept while it is reversed
+    size_t tmp_bytes = 0;
+    char *ckpt = nullptr;          // checkpoints of the window (segment starts, then the end)
+    size_t ckpt_bytes = 0;
+    char *undo = nullptr;          // undo logs of one segment's cycles
+    size_t undo_bytes = 0;
+    double *mis = nullptr;         // misfit: J, column heights, target, weights
+    size_t mis_doubles = 0;
+};
+
+namespace {
+
+// fields a cycle writes and later cycles or sweeps read (state of a checkpoint); the face
+// records and the pure transients are rewritten before they are read
+const char *const kAdjSnapshot[] = {"e_ejt", "m_vof", "e_dvel", "e_den", "v_vof", "v_vel", "v_mass", "e_vel",
+                                    "e_grad_vel", "e_div_vel", "e_q", "e_ste", "e_ste2s", "e_sta2s", "e_tps", "e_dam",
+                                    "e_strength", "e_vib", "e_pre", "v_acc", "v_alpha", "v_dis", "m_eng", "e_cvs",
+                                    "m_pty", "e_wpt", "m_den", "e_cnd", "e_csd", "e_tem", "e_mu", "e_alpha", "e_beta",
+                                    "y_profile"};
+// fields each phase writes (its undo log), face records excepted: every face is rewritten by its
+// donor cell in phase 12 before phase 14 reads it
+const std::vector<const char *> kAdjWrites[16] = {
+    {"y_profile", "e_ejt"},
+    {"m_vof", "e_dvel", "e_den", "v_vof", "v_vel", "v_mass"},
+    {},
+    {"e_vel"},
+    {"v_vel"},
+    {"e_grad_vel", "e_div_vel", "e_q"},
+    {},
+    {"e_ste", "e_ste2s", "e_sta2s", "e_tps", "e_dam", "e_strength", "e_vib"},
+    {"e_pre", "e_ste", "e_q", "v_acc", "v_alpha"},
+    {"v_dis", "v_vel"},
+    {"m_eng", "e_cvs", "m_pty"},
+    {},
+    {"e_wpt", "m_den", "e_vib", "m_eng", "m_pty", "e_cvs"},
+    {"e_cnd"},
+    {"m_vof", "m_den", "m_eng", "m_pty", "e_dvel", "e_ste", "e_dam", "e_tps", "e_vib", "e_ejt", "e_den", "e_pre",
+     "e_csd", "e_tem", "e_mu", "e_alpha", "e_beta", "e_cvs"},
+    {},
+};
+
+size_t field_bytes(const salec_gpu *h, int k)
+{
+    const size_t col = (((size_t)h->d.enx + 31) / 32) * 32;
+    return kFields[k].loc == L_COL ? col * sizeof(double) : (size_t)field_ncomp(h, k) * h->d.PL * field_elem(h, k);
+}
+
+template <class List>
+size_t list_bytes(const salec_gpu *h, const List &names)
+{
+    size_t b = sizeof(Scal);
+    for (const char *n : names) b += field_bytes(h, field_by_name(n));
+    return (b + 255) & ~(size_t)255;
+}
+
+// copy the listed fields and the scalar block to (save) or from (restore) buf
+template <class List>
+int copy_list(salec_gpu *h, const List &names, char *buf, bool save)
+{
+    size_t off = 0;
+    for (const char *n : names) {
+        const int k = field_by_name(n);
+        const size_t nb = field_bytes(h, k);
+        char *f = reinterpret_cast<char *>(field_ptr(h, k));
+        CUDA_TRY(cudaMemcpyAsync(save ? buf + off : f, save ? f : buf + off, nb, cudaMemcpyDeviceToDevice, h->stream));
+        off += nb;
+    }
+    CUDA_TRY(cudaMemcpyAsync(save ? buf + off : reinterpret_cast<char *>(h->scal),
+                             save ? reinterpret_cast<char *>(h->scal) : buf + off, sizeof(Scal),
+                             cudaMemcpyDeviceToDevice, h->stream));
+    return SALEC_OK;
+}
+
+void adjoint_release(salec_gpu *h)
+{
+    AdjointState *st = h->adj;
+    if (!st) return;
+    cudaFree(st->pool);
+    cudaFree(st->theta);
+    cudaFree(st->gscratch);
+    cudaFree(st->tmp);
+    cudaFree(st->ckpt);
+    cudaFree(st->undo);
+    cudaFree(st->mis);
+    delete st;
+    h->adj = nullptr;
+}
+
+const char *adjoint_unsupported(const salec_gpu *h, const DevMat &m1)
+{
+    if (h->mixed) return "the adjoint runs on the plain FP64 form";
+    if (h->d.nmat != 2) return "the adjoint supports one material beside vacuum";
+    if (h->rp.damp_type != 5) return "the adjoint supports damping = none";
+    if (h->rp.porosity_model || h->rp.acoustic_fluid || h->rp.tensile_failure || h->rp.tracer_lubrication > 0)
+        return "the adjoint supports no porosity, acoustic fluidisation, tensile failure or tracer lubrication";
+    if (h->rp.flow_resistance > 0. || h->rp.flow_friction > 0.) return "the adjoint supports no ejecta drag";
+    if (h->rp.partpres) return "the adjoint supports partpres = 0";
+    if (m1.eos_type != SALEC_EOS_TILLOTSON) return "the adjoint supports a Tillotson material";
+    if (m1.yfunc != SALEC_FN_ROCK_STRENGTH_T) return "the adjoint supports the RockStrengthT yield model";
+    if (m1.dsdf != SALEC_FN_IVANOV && m1.dsdf != SALEC_FN_SIMPLE_SHEAR) return "the adjoint supports Ivanov damage";
+    if (m1.PolyLiq > 0 || m1.PolySol > 0) return "the adjoint supports the Simon melting curve only";
+    return nullptr;
+}
+
+int adjoint_ensure(salec_gpu *h)
+{
+    if (!h->adj) h->adj = new AdjointState();
+    AdjointState *st = h->adj;
+    if (!st->pool) {
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->pool), h->pool_bytes));
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->theta), 4 * sizeof(double)));
+        for (int k = 0; k < kNumFields; ++k) {
+            const size_t off = reinterpret_cast<char *>(field_ptr(h, k)) - h->pool;
+            *reinterpret_cast<double **>(reinterpret_cast<char *>(&st->b) + kFields[k].off) =
+                reinterpret_cast<double *>(st->pool + off);
+        }
+        size_t gs = 0;
+        for (const Gather *g : {&h->g_mvof, &h->g_dvel_den, &h->g_evel, &h->g_pre_ste_q, &h->g_flux_state, &h->r_vel,
+                                &h->r_acc, &h->r_dis}) {
+            size_t e = 0;
+            for (int f = 0; f < g->batch.nfield; ++f) e += g->entries[f];
+            gs = std::max(gs, e * (size_t)std::max(g->ncomp_max, 1));
+        }
+        st->gscratch_doubles = std::max<size_t>(gs, 1);
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->gscratch), st->gscratch_doubles * sizeof(double)));
+        size_t tb = 0;
+        for (int p = 0; p < 16; ++p) tb = std::max(tb, list_bytes(h, kAdjWrites[p]));
+        st->tmp_bytes = tb;
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->tmp), tb));
+    }
+    return SALEC_OK;
+}
+
+int adjoint_zero(salec_gpu *h)
+{
+    CUDA_TRY(cudaMemsetAsync(h->adj->pool, 0, h->pool_bytes, h->stream));
+    CUDA_TRY(cudaMemsetAsync(h->adj->theta, 0, 4 * sizeof(double), h->stream));
+    return SALEC_OK;
+}
+
+int adjoint_gather(salec_gpu *h, const Gather &g)
+{
+    if (g.batch.total == 0) return SALEC_OK;
+    const void *adj[SALEC_MAX_GATHER_FIELDS];
+    for (int f = 0; f < g.batch.nfield; ++f)
+        adj[f] = h->adj->pool + (static_cast<char *>(g.batch.field[f].base) - h->pool);
+    launch_adjoint_gather(g.batch, g.entries, adj, h->adj->gscratch, h->stream);
+    CUDA_TRY(cudaGetLastError());
+    return SALEC_OK;
+}
+
+// Reverse of phase p with the current field pool as the state before phase p (left so on return).
+int adjoint_phase(salec_gpu *h, int p, double dt)
+{
+    AdjointState *st = h->adj;
+    AdjCtx a;
+    a.c = h->ctx();
+    a.b = st->b;
+    a.dt = dt;
+    a.theta = st->theta;
+    cudaStream_t s = h->stream;
+    const Ctx &c = a.c;
+    auto keep = [&](std::initializer_list<const char *> names, bool save) {
+        return copy_list(h, std::vector<const char *>(names), st->tmp, save);
+    };
+    int rc = SALEC_OK;
+    switch (p) {
+    case 14: launch_adjoint_kernel(AK_REMAP_STATE, a, s); break;
+    case 12:
+        if ((rc = keep({"m_den", "e_vib", "m_eng"}, true))) return rc;
+        if ((rc = run_gather(h, h->g_flux_state))) return rc;
+        launch_adjoint_kernel(AK_FLUX, a, s);
+        if ((rc = keep({"m_den", "e_vib", "m_eng"}, false))) return rc;
+        if ((rc = adjoint_gather(h, h->g_flux_state))) return rc;
+        break;
+    case 10: launch_adjoint_kernel(AK_ENERGY, a, s); break;
+    case 9:
+        if ((rc = keep({"v_dis", "v_vel"}, true))) return rc;
+        launch_step_kernel(SK_DISPLACEMENT, c, s, h->blk[SK_DISPLACEMENT]);
+        if ((rc = adjoint_gather(h, h->r_dis))) return rc;
+        if ((rc = keep({"v_dis", "v_vel"}, false))) return rc;
+        launch_adjoint_kernel(AK_DISPLACEMENT, a, s);
+        break;
+    case 8:
+        if ((rc = keep({"e_pre", "e_ste", "e_q", "v_acc"}, true))) return rc;
+        if ((rc = run_gather(h, h->g_pre_ste_q))) return rc;
+        launch_step_kernel(SK_ACCELERATION, c, s, h->blk[SK_ACCELERATION]);
+        if ((rc = adjoint_gather(h, h->r_acc))) return rc;
+        launch_adjoint_kernel(AK_ACCELERATION, a, s);
+        if ((rc = keep({"e_pre", "e_ste", "e_q", "v_acc"}, false))) return rc;
+        if ((rc = adjoint_gather(h, h->g_pre_ste_q))) return rc;
+        break;
+    case 7: launch_adjoint_kernel(AK_STRESS, a, s); break;
+    case 5: launch_adjoint_kernel(AK_GRADIENT, a, s); break;
+    case 4: launch_adjoint_kernel(AK_VOID_VERTICES, a, s); break;
+    case 3:
+        if ((rc = keep({"e_vel"}, true))) return rc;
+        launch_step_kernel(SK_CELL_VELOCITY, c, s, h->blk[SK_CELL_VELOCITY]);
+        if ((rc = adjoint_gather(h, h->g_evel))) return rc;
+        if ((rc = keep({"e_vel"}, false))) return rc;
+        launch_adjoint_kernel(AK_CELL_VELOCITY, a, s);
+        break;
+    case 1: {
+        if ((rc = keep({"m_vof", "e_dvel", "e_den", "v_vof", "v_vel", "v_mass"}, true))) return rc;
+        if ((rc = run_gather(h, h->g_mvof))) return rc;
+        if ((rc = run_gather(h, h->g_dvel_den))) return rc;
+        launch_step_kernel(SK_VERTEX_VOF_MOMENTUM, c, s, h->blk[SK_VERTEX_VOF_MOMENTUM]);
+        if ((rc = adjoint_gather(h, h->r_vel))) return rc;
+        // back to the gathered cell fields with the vertex fields before the sweep
+        size_t off = 0;
+        for (const char *n : {"m_vof", "e_dvel", "e_den"}) off += field_bytes(h, field_by_name(n));
+        for (const char *n : {"v_vof", "v_vel", "v_mass"}) {
+            const int k = field_by_name(n);
+            const size_t nb = field_bytes(h, k);
+            CUDA_TRY(cudaMemcpyAsync(field_ptr(h, k), st->tmp + off, nb, cudaMemcpyDeviceToDevice, s));
+            off += nb;
+        }
+        launch_adjoint_kernel(AK_VERTEX_MOMENTUM, a, s);
+        if ((rc = keep({"m_vof", "e_dvel", "e_den", "v_vof", "v_vel", "v_mass"}, false))) return rc;
+        if ((rc = adjoint_gather(h, h->g_dvel_den))) return rc;
+        if ((rc = adjoint_gather(h, h->g_mvof))) return rc;
+        break;
+    }
+    default: break;   // phases 0, 2, 6, 11, 13 and 15 write nothing an adjoint flows through
+    }
+    CUDA_TRY(cudaGetLastError());
+    return SALEC_OK;
+}
+
+int adjoint_transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
+{
+    double *&slot = field_ptr(h, fid);
+    double *saved = slot;
+    slot = reinterpret_cast<double *>(h->adj->pool + (reinterpret_cast<char *>(saved) - h->pool));
+    int rc = SALEC_OK;
+    // the conversion only; the geometry tables and the Laplacian mask of the forward fields stay
+    int nx, ny;
+    field_points(h, fid, nx, ny);
+    const int nc = field_ncomp(h, fid);
+    const long long need = (long long)nx * ny * nc;
+    if (n != need) rc = fail(SALEC_ERR_ARG, std::string("adjoint field ") + kFields[fid].name + ": expected " +
+                                                 std::to_string(need) + " doubles");
+    else if ((rc = ensure_staging(h, (size_t)need)) == SALEC_OK) {
+        const long long plane = kFields[fid].loc == L_COL ? 0 : h->d.PL;
+        cudaError_t e;
+        if (to_device) {
+            e = cudaMemcpyAsync(h->staging, host, need * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+            if (e == cudaSuccess) launch_aos_to_planes(h->staging, slot, false, plane, h->d.P, nx, ny, nc, h->stream);
+        } else {
+            launch_planes_to_aos(slot, false, h->staging, plane, h->d.P, nx, ny, nc, h->stream);
+            e = cudaMemcpyAsync(host, h->staging, need * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) rc = fail(SALEC_ERR_CUDA, std::string("adjoint transfer: ") + cudaGetErrorString(e));
+    }
+    slot = saved;
+    return rc;
+}
+
+int adjoint_check(salec_gpu *h)
+{
+    DevMat m1;
+    if (cudaMemcpy(&m1, h->mat + 1, sizeof(DevMat), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(SALEC_ERR_CUDA, "material read-back");
+    if (const char *why = adjoint_unsupported(h, m1)) return fail(SALEC_ERR_UNSUPPORTED, why);
+    return adjoint_ensure(h);
+}
+
+} // namespace
+
+extern "C" {
+
+int salec_gpu_set_dt_schedule(salec_gpu *h, const double *dts, int n)
+{
+    if (!h || n < 0 || (n > 0 && !dts)) return fail(SALEC_ERR_ARG, "bad argument");
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->dt_sched) CUDA_TRY(cudaFree(h->dt_sched));
+    h->dt_sched = nullptr;
+    h->dt_sched_n = 0;
+    if (n > 0) {
+        CUDA_TRY(cudaMemcpy(&h->scal_host->i_step, &h->scal->i_step, sizeof(long long), cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&h->dt_sched), n * sizeof(double)));
+        CUDA_TRY(cudaMemcpy(h->dt_sched, dts, n * sizeof(double), cudaMemcpyHostToDevice));
+        h->dt_sched_i0 = h->scal_host->i_step;
+        h->dt_sched_n = n;
+    }
+    drop_cycle_graph(h);
+    return SALEC_OK;
+}
+
+int salec_gpu_adjoint_reset(salec_gpu *h)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    if (int rc = adjoint_check(h)) return rc;
+    if (int rc = adjoint_zero(h)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return SALEC_OK;
+}
+
+int salec_gpu_adjoint_set_field(salec_gpu *h, int field, const double *host, long long n)
+{
+    if (!h || !host || !h->adj || !h->adj->pool) return fail(SALEC_ERR_STATE, "call salec_gpu_adjoint_reset first");
+    if (field < 0 || field >= kNumFields) return fail(SALEC_ERR_ARG, "unknown field");
+    return adjoint_transfer(h, field, const_cast<double *>(host), n, true);
+}
+
+int salec_gpu_adjoint_get_field(salec_gpu *h, int field, double *host, long long n)
+{
+    if (!h || !host || !h->adj || !h->adj->pool) return fail(SALEC_ERR_STATE, "call salec_gpu_adjoint_reset first");
+    if (field < 0 || field >= kNumFields) return fail(SALEC_ERR_ARG, "unknown field");
+    return adjoint_transfer(h, field, host, n, false);
+}
+
+int salec_gpu_adjoint_phase(salec_gpu *h, int phase)
+{
+    if (!h || !h->adj || !h->adj->pool) return fail(SALEC_ERR_STATE, "call salec_gpu_adjoint_reset first");
+    if (phase < 0 || phase > 15) return fail(SALEC_ERR_ARG, "phase out of range");
+    CUDA_TRY(cudaMemcpy(h->scal_host, h->scal, sizeof(Scal), cudaMemcpyDeviceToHost));
+    if (int rc = adjoint_phase(h, phase, h->scal_host->dt)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return SALEC_OK;
+}
+
+int salec_gpu_adjoint_params(salec_gpu *h, double *theta)
+{
+    if (!h || !theta || !h->adj || !h->adj->pool) return fail(SALEC_ERR_STATE, "call salec_gpu_adjoint_reset first");
+    CUDA_TRY(cudaMemcpyAsync(theta, h->adj->theta, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return SALEC_OK;
+}
+
+int salec_gpu_adjoint_window(salec_gpu *h, int nsteps, int every, const double *target, const double *weight,
+                             int ncols, double *grad_density, long long n_density, salec_adjoint_result *out)
+{
+    if (!h || nsteps < 1 || every < 1 || !target || !out) return fail(SALEC_ERR_ARG, "bad argument");
+    if (ncols != h->d.enx - 4) return fail(SALEC_ERR_ARG, "target and weights need one value per interior column");
+    if (grad_density && n_density != (long long)h->d.enx * h->d.eny)
+        return fail(SALEC_ERR_ARG, "grad_density needs (nx+4)*(ny+4) doubles");
+    if (int rc = adjoint_check(h)) return rc;
+    AdjointState *st = h->adj;
+    cudaStream_t s = h->stream;
+    const int nseg = (nsteps + every - 1) / every;
+    const std::vector<const char *> snap(std::begin(kAdjSnapshot), std::end(kAdjSnapshot));
+    const size_t sb = list_bytes(h, snap);
+    size_t ub = 0;
+    std::vector<size_t> uoff(16);
+    for (int p = 0; p < 16; ++p) { uoff[p] = ub; ub += list_bytes(h, kAdjWrites[p]); }
+    // buffers: nseg + 1 checkpoints (the last is the window's end), `every` undo logs
+    const size_t need_ck = sb * (nseg + 1), need_ud = ub * every;
+    if (st->ckpt_bytes < need_ck) {
+        cudaFree(st->ckpt);
+        st->ckpt = nullptr;
+        st->ckpt_bytes = 0;
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->ckpt), need_ck));
+        st->ckpt_bytes = need_ck;
+    }
+    if (st->undo_bytes < need_ud) {
+        cudaFree(st->undo);
+        st->undo = nullptr;
+        st->undo_bytes = 0;
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->undo), need_ud));
+        st->undo_bytes = need_ud;
+    }
+    const size_t md = 1 + 3 * (size_t)ncols;
+    if (st->mis_doubles < md) {
+        cudaFree(st->mis);
+        st->mis = nullptr;
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->mis), md * sizeof(double)));
+        st->mis_doubles = md;
+    }
+    std::vector<double> dts(nsteps);
+    // forward window, with a checkpoint at every segment start
+    for (int sgm = 0; sgm < nseg; ++sgm) {
+        if (int rc = copy_list(h, snap, st->ckpt + sb * sgm, true)) return rc;
+        const int n = std::min(every, nsteps - sgm * every);
+        for (int k = 0; k < n; ++k) {
+            if (int rc = salec_gpu_step(h, 1)) return rc;
+            CUDA_TRY(cudaMemcpyAsync(&dts[sgm * every + k], &h->scal->dt, sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+    }
+    if (int rc = copy_list(h, snap, st->ckpt + sb * nseg, true)) return rc;
+    // the tracers are not part of the differentiated state: the replays move them, so the end's
+    // are kept and put back
+    std::vector<char> tr_end(h->tr_bytes);
+    if (h->tr_bytes) {
+        CUDA_TRY(cudaStreamSynchronize(s));
+        CUDA_TRY(cudaMemcpy(tr_end.data(), h->tr_block, h->tr_bytes, cudaMemcpyDeviceToHost));
+    }
+    // misfit of the final surface profile and the seed of the reverse sweep
+    if (int rc = adjoint_zero(h)) return rc;
+    std::vector<double> w(ncols, 1.0);
+    if (weight) w.assign(weight, weight + ncols);
+    CUDA_TRY(cudaMemsetAsync(st->mis, 0, sizeof(double), s));
+    CUDA_TRY(cudaMemcpyAsync(st->mis + 1 + ncols, target, ncols * sizeof(double), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(st->mis + 1 + 2 * ncols, w.data(), ncols * sizeof(double), cudaMemcpyHostToDevice, s));
+    launch_profile_misfit(h->ctx(), st->b, st->mis + 1 + ncols, st->mis + 1 + 2 * ncols, st->mis, st->mis + 1, s);
+    CUDA_TRY(cudaGetLastError());
+    double J = 0.;
+    CUDA_TRY(cudaMemcpyAsync(&J, st->mis, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    // reverse: per segment, replay its cycles from the checkpoint with undo logs, then walk back
+    for (int sgm = nseg - 1; sgm >= 0; --sgm) {
+        if (int rc = copy_list(h, snap, st->ckpt + sb * sgm, false)) return rc;
+        const int n = std::min(every, nsteps - sgm * every);
+        for (int k = 0; k < n; ++k) {
+            char *log = st->undo + ub * k;
+            for (int p = 0; p <= 15; ++p) {
+                if (int rc = copy_list(h, kAdjWrites[p], log + uoff[p], true)) return rc;
+                if (int rc = run_phase(h, p)) return rc;
+            }
+        }
+        for (int k = n - 1; k >= 0; --k) {
+            char *log = st->undo + ub * k;
+            const double dt = dts[sgm * every + k];
+            for (int p = 15; p >= 0; --p) {
+                if (int rc = copy_list(h, kAdjWrites[p], log + uoff[p], false)) return rc;
+                if (int rc = adjoint_phase(h, p, dt)) return rc;
+            }
+        }
+    }
+    // the pool now holds the window's start and the adjoint planes its sensitivities
+    out->misfit = J;
+    CUDA_TRY(cudaMemcpyAsync(out->d_params, st->theta, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    {
+        const int fv = field_by_name("v_vel");
+        int nx, ny;
+        field_points(h, fv, nx, ny);
+        const long long nv = (long long)nx * ny * 2;
+        std::vector<double> v(nv), bv(nv);
+        if (int rc = transfer(h, fv, v.data(), nv, false)) return rc;
+        if (int rc = adjoint_transfer(h, fv, bv.data(), nv, false)) return rc;
+        double sv = 0.;
+        for (long long q = 0; q < nv; ++q) sv += bv[q] * v[q];
+        out->d_velocity_scale = sv;
+    }
+    if (grad_density) {
+        const int fm = field_by_name("m_den"), fe = field_by_name("e_den");
+        const long long nc = (long long)h->d.enx * h->d.eny;
+        std::vector<double> md2(nc * 2), bm(nc * 2), ed(nc), be(nc);
+        if (int rc = transfer(h, fm, md2.data(), nc * 2, false)) return rc;
+        if (int rc = adjoint_transfer(h, fm, bm.data(), nc * 2, false)) return rc;
+        if (int rc = transfer(h, fe, ed.data(), nc, false)) return rc;
+        if (int rc = adjoint_transfer(h, fe, be.data(), nc, false)) return rc;
+        for (long long q = 0; q < nc; ++q) {
+            const double g = bm[2 * q] * md2[2 * q] + bm[2 * q + 1] * md2[2 * q + 1] + be[q] * ed[q];
+            grad_density[q] = ed[q] > 0.0 ? g / ed[q] : 0.0;
+        }
+    }
+    // leave the simulation at the end of the window
+    if (int rc = copy_list(h, snap, st->ckpt + sb * nseg, false)) return rc;
+    if (h->tr_bytes) CUDA_TRY(cudaMemcpy(h->tr_block, tr_end.data(), h->tr_bytes, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return SALEC_OK;
 }
 
 } // extern "C"

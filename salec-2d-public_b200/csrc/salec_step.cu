@@ -351,16 +351,17 @@ __global__ void k_void_vertices(const CtxT<R> c)
 template <class R>
 __global__ void SALEC_BOUNDS_GRAD k_gradient_viscosity_cfl(const CtxT<R> c)
 {
+    using A = R;   // arithmetic of the gradient and the viscosity: FP64, or FP32 in the mixed form
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     unsigned long long cand = ~0ULL;
     if (cell_interior(c, i, j)) {
         const long long p = KIDX(i, j);
         const long long vl[4] = {KIDX(i, j), KIDX(i + 1, j), KIDX(i + 1, j + 1), KIDX(i, j + 1)};
-        double vx[4], vy[4];
+        A vx[4], vy[4];
         for (int k = 0; k < 4; ++k) { vx[k] = c.f.v_vel[vl[k]]; vy[k] = PLN(c.f.v_vel, 1)[vl[k]]; }
-        double g[12];
+        A g[12];
         for (int k = 0; k < 12; ++k) g[k] = GEO(c.g_e_grad, k);
-        double d0 = 0., d1 = 0., d2 = 0., d3 = 0., d4 = 0.;
+        A d0 = A(0.), d1 = A(0.), d2 = A(0.), d3 = A(0.), d4 = A(0.);
         for (int k = 0; k < 4; ++k) d0 += g[k] * vx[k];        // dv_r/dr
         for (int k = 0; k < 4; ++k) d2 += g[k] * vy[k];        // dv_z/dr
         for (int k = 0; k < 4; ++k) d1 += g[4 + k] * vx[k];    // dv_r/dz
@@ -371,26 +372,26 @@ __global__ void SALEC_BOUNDS_GRAD k_gradient_viscosity_cfl(const CtxT<R> c)
         PLN(c.f.e_grad_vel, 2)[p] = d2;
         PLN(c.f.e_grad_vel, 3)[p] = d3;
         PLN(c.f.e_grad_vel, 4)[p] = d4;
-        const double div = d0 + d3 + d4;
+        const A div = d0 + d3 + d4;
         c.f.e_div_vel[p] = div;
         const double vof0 = c.f.m_vof[p];
-        const double csd = c.f.e_csd[p];
-        double q;
-        if (vof0 > SALEC_TOLVOF || c.f.e_pre[p] <= 0.0) {
-            q = 0.;
+        const A csd = c.f.e_csd[p];
+        A q;
+        if (vof0 > SALEC_TOLVOF || c.f.e_pre[p] <= A(0.0)) {
+            q = A(0.);
         } else {
-            double area = GEO(c.g_e_vol, 0) / c.f.e_pos[p];
-            area = fabs(area);
-            const double ql = c.rp.avis1 * csd * sqrt(area);
-            const double qq = c.rp.avis2 * div * area;
-            q = dmin(0., div) * c.f.e_den[p] * (qq - ql);
-            if (q < SALEC_TOLQPRE) q = 0.;
+            double aread = GEO(c.g_e_vol, 0) / c.f.e_pos[p];
+            const A area = A(fabs(aread));
+            const A ql = A(c.rp.avis1) * csd * sqrt(area);
+            const A qq = A(c.rp.avis2) * div * area;
+            q = amin(A(0.), div) * A(c.f.e_den[p]) * (qq - ql);
+            if (q < A(SALEC_TOLQPRE)) q = A(0.);
         }
         c.f.e_q[p] = q;
-        // CFL candidate over cells that are not pure vacuum; a NaN candidate is recorded by its
-        // position in the reference's traversal order instead (see k_finalize_dt)
+        // CFL candidate over cells that are not pure vacuum, in FP64; a NaN candidate is recorded
+        // by its position in the reference's traversal order instead (see k_finalize_dt)
         if (!(vof0 > 1.0 - SALEC_TOLVOF)) {
-            const double dt_rz = cfl_candidate(c, p, csd);
+            const double dt_rz = cfl_candidate(c, p, (double)csd);
             if (dt_rz == dt_rz) cand = ord_encode(dt_rz);
             else atomicMax(&c.scal->dt_nan_last, (long long)j * c.d.enx + i);
         }
@@ -410,7 +411,8 @@ __global__ void SALEC_BOUNDS_GRAD k_gradient_viscosity_cfl(const CtxT<R> c)
     }
 }
 
-// phase 6: dt of this cycle. The reference folds the candidates in traversal order (j outer, i
+// phase 6: dt of this cycle: a prescribed time step where the handle has a schedule for this
+// cycle (salec_gpu_set_dt_schedule), else the CFL reduction. The reference folds the candidates in traversal order (j outer, i
 // inner) with MIN(a, b) = a < b ? a : b (src/mpi_vec/mpi_vec_types.h:262), starting from
 // 1.1 * dt_prev: a NaN candidate makes the running value NaN, and the next candidate replaces
 // it. So with no NaN the result is the order-free MIN of the gradient sweep; otherwise it is
@@ -421,6 +423,13 @@ __global__ void SALEC_BOUNDS_GRAD k_gradient_viscosity_cfl(const CtxT<R> c)
 template <class R>
 __global__ void __launch_bounds__(SALEC_FINALIZE_THREADS) k_finalize_dt(const CtxT<R> c)
 {
+    if (c.dt_sched) {
+        const long long k = c.scal->i_step - c.dt_sched_i0;
+        if (k >= 0 && k < c.dt_sched_n) {
+            if (threadIdx.x == 0 && blockIdx.x == 0) c.scal->dt = c.dt_sched[k];
+            return;
+        }
+    }
     const long long last = c.scal->dt_nan_last;
     if (last < 0) {
         if (threadIdx.x == 0 && blockIdx.x == 0) c.scal->dt = step_dt(c);
@@ -460,45 +469,46 @@ __global__ void __launch_bounds__(SALEC_FINALIZE_THREADS) k_finalize_dt(const Ct
 template <class R, int NM, bool POR>
 __global__ void SALEC_BOUNDS_STRESS k_stress(const CtxT<R> c)
 {
+    using A = R;   // arithmetic of stress, strength and damage: FP64, or FP32 in the mixed form
     constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!cell_interior(c, i, j)) return;
     const long long p = KIDX(i, j);
     const int nmat = NM > 0 ? NM : c.d.nmat;
-    const double dt = c.scal->dt;
+    const A dt = A(c.scal->dt);
     const double vof0 = c.f.m_vof[p];
-    double dam = c.f.e_dam[p];
+    A dam = c.f.e_dam[p];
 
     // --- acoustic fluidisation (block model)
     if (c.rp.acoustic_fluid) {
-        double vib = c.f.e_vib[p];
-        if (vof0 > SALEC_TOLVOF || dam < 0.5) {
-            vib = 0.;
+        A vib = c.f.e_vib[p];
+        if (vof0 > SALEC_TOLVOF || dam < A(0.5)) {
+            vib = A(0.);
         } else {
-            double tdec = -1.0, cvib = 0.0, toff = -1.0, vmax = 0.0, pvl = 0.0;
+            A tdec = A(-1.0), cvib = A(0.0), toff = A(-1.0), vmax = A(0.0), pvl = A(0.0);
             for (int m = 1; m < nmat; ++m) {
                 if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
                 const DevMat &s = c.mat[m];
-                tdec = dmax(s.Tdamp, tdec);
-                cvib = dmax(s.Cvib, cvib);
-                toff = dmax(s.Toff, toff);
-                vmax = dmax(s.VibMax, vmax);
-                pvl = dmax(s.Pvlim, pvl);
+                tdec = amax(A(s.Tdamp), tdec);
+                cvib = amax(A(s.Cvib), cvib);
+                toff = amax(A(s.Toff), toff);
+                vmax = amax(A(s.VibMax), vmax);
+                pvl = amax(A(s.Pvlim), pvl);
             }
-            if (tdec <= 0. || toff <= 0.) {
-                vib = 0.;
+            if (tdec <= A(0.) || toff <= A(0.)) {
+                vib = A(0.);
             } else {
-                const double evx = c.f.e_vel[p], evy = PLN(c.f.e_vel, 1)[p];
-                double len = 0.;
+                const A evx = c.f.e_vel[p], evy = PLN(c.f.e_vel, 1)[p];
+                A len = A(0.);
                 len += evx * evx;
                 len += evy * evy;
-                const double nv = cvib * sqrt(len);
-                const double nv2 = nv * nv;
-                const double t = c.scal->time;
-                if ((t <= toff) && (nv2 >= vib) && (nv >= 1.0) && (c.f.e_q[p] > 0.))
-                    vib = dmin(nv2, vmax * vmax);
+                const A nv = cvib * sqrt(len);
+                const A nv2 = nv * nv;
+                const A t = A(c.scal->time);
+                if ((t <= toff) && (nv2 >= vib) && (nv >= A(1.0)) && (c.f.e_q[p] > A(0.)))
+                    vib = amin(nv2, vmax * vmax);
                 else
-                    vib = dmax(vib * (1.0 - 2.0 * dt / tdec + 2.0 * (dt / tdec) * (dt / tdec)), 0.0);
+                    vib = amax(vib * (A(1.0) - A(2.0) * dt / tdec + A(2.0) * (dt / tdec) * (dt / tdec)), A(0.0));
             }
         }
         c.f.e_vib[p] = vib;
@@ -511,80 +521,80 @@ __global__ void SALEC_BOUNDS_STRESS k_stress(const CtxT<R> c)
         return;
     }
     // every input of a full cell, issued in one batch
-    double s0 = c.f.e_ste[p], s1 = PLN(c.f.e_ste, 1)[p], s2 = PLN(c.f.e_ste, 2)[p], s3 = PLN(c.f.e_ste, 3)[p];
-    double ste2s = c.f.e_ste2s[p], sta2s = c.f.e_sta2s[p], tps = c.f.e_tps[p], strength = c.f.e_strength[p];
-    double vmat[MM], ptm[MM];
+    A s0 = c.f.e_ste[p], s1 = PLN(c.f.e_ste, 1)[p], s2 = PLN(c.f.e_ste, 2)[p], s3 = PLN(c.f.e_ste, 3)[p];
+    A ste2s = c.f.e_ste2s[p], sta2s = c.f.e_sta2s[p], tps = c.f.e_tps[p], strength = c.f.e_strength[p];
+    A vmat[MM], ptm[MM];
     #pragma unroll
     for (int m = 1; m < nmat; ++m) {
-        vmat[m] = PLN(c.f.m_vof, m)[p];
-        ptm[m] = POR ? PLN(c.f.m_pty, m)[p] : 1.0;
+        vmat[m] = A(PLN(c.f.m_vof, m)[p]);
+        ptm[m] = POR ? A(PLN(c.f.m_pty, m)[p]) : A(1.0);
     }
-    const double rho = c.f.e_den[p];
-    const double g0 = c.f.e_grad_vel[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
-                 g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
-    const double mu = c.f.e_mu[p];
-    const double pre = c.f.e_pre[p], tem = c.f.e_tem[p], csd = c.f.e_csd[p];
-    double vapor_ref = 0., melt_ref = 0.;
+    const A rho = c.f.e_den[p];
+    const A g0 = c.f.e_grad_vel[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
+            g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
+    const A mu = c.f.e_mu[p];
+    const A pre = c.f.e_pre[p], tem = c.f.e_tem[p], csd = c.f.e_csd[p];
+    A vapor_ref = A(0.), melt_ref = A(0.);
     #pragma unroll
     for (int m = 1; m < nmat; ++m) {
-        const double vm = vmat[m];
-        if (vm < SALEC_TOLVOF) continue;
-        vapor_ref += vm * c.mat[m].VaporDen;
-        melt_ref += vm * c.mat[m].MeltDen;
+        const A vm = vmat[m];
+        if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
+        vapor_ref += vm * A(c.mat[m].VaporDen);
+        melt_ref += vm * A(c.mat[m].MeltDen);
     }
-    double porosity = 0.0;
+    A porosity = A(0.0);
     if (POR) {
-        double mv = 0.0;
+        A mv = A(0.0);
         #pragma unroll
         for (int m = 1; m < nmat; ++m) {
-            const double vm = vmat[m];
-            if (vm < SALEC_TOLVOF) continue;
+            const A vm = vmat[m];
+            if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
             porosity += vm * ptm[m];
             mv += vm;
         }
         porosity /= mv;
     } else {
-        porosity = 1.0;
+        porosity = A(1.0);
     }
-    porosity = dmax(porosity, 1.0);
+    porosity = amax(porosity, A(1.0));
     vapor_ref /= porosity;
     melt_ref /= porosity;
 
-    const double ste2s_old = ste2s;
+    const A ste2s_old = ste2s;
     int state; // 0 solid, 1 melt, 2 vapour
     if (rho <= vapor_ref) {
         state = 2;
-        s0 = s1 = s2 = s3 = 0.;
-        ste2s = 0.;
-        tps = 0.;
-        dam = 0.;
-        strength = 0.;
+        s0 = s1 = s2 = s3 = A(0.);
+        ste2s = A(0.);
+        tps = A(0.);
+        dam = A(0.);
+        strength = A(0.);
     } else {
-        double e0 = g0, e1 = 0.5 * g1 + 0.5 * g2, e2 = g3, e3 = g4;
-        const double tr = e0 + e2 + e3;
-        e0 -= tr / 3.0;
-        e2 -= tr / 3.0;
-        e3 -= tr / 3.0;
+        A e0 = g0, e1 = A(0.5) * g1 + A(0.5) * g2, e2 = g3, e3 = g4;
+        const A tr = e0 + e2 + e3;
+        e0 -= tr / A(3.0);
+        e2 -= tr / A(3.0);
+        e3 -= tr / A(3.0);
         if (rho <= melt_ref) {
             state = 1;
-            s0 = s1 = s2 = s3 = 0.;
-            ste2s = 0.;
+            s0 = s1 = s2 = s3 = A(0.);
+            ste2s = A(0.);
             sta2s = sqrt(second_inv(e0, e1, e2, e3));
-            tps = dmin(tps + sta2s * dt, 10.);
-            dam = 1.;
-            strength = 0.;
+            tps = amin(tps + sta2s * dt, A(10.));
+            dam = A(1.);
+            strength = A(0.);
         } else {
             state = 0;
             // Wilkins rotation
-            double sin2o = (g2 - g1) * dt;
-            sin2o = wind(sin2o, -1., 1.);
-            const double cos2o1 = sqrt(1.0 - sin2o * sin2o) - 1.0;
-            const double ss2 = (s0 - s2) / 2.0;
-            const double r0 = ss2 * cos2o1 + s1 * sin2o;
-            const double r1 = s1 * cos2o1 - ss2 * sin2o;
-            const double r2 = -ss2 * cos2o1 - s1 * sin2o;
-            s0 += 1.0 * r0; s1 += 1.0 * r1; s2 += 1.0 * r2; s3 += 1.0 * 0.0;
-            const double k2 = 2.0 * mu * dt;
+            A sin2o = (g2 - g1) * dt;
+            sin2o = awind(sin2o, A(-1.), A(1.));
+            const A cos2o1 = sqrt(A(1.0) - sin2o * sin2o) - A(1.0);
+            const A ss2 = (s0 - s2) / A(2.0);
+            const A r0 = ss2 * cos2o1 + s1 * sin2o;
+            const A r1 = s1 * cos2o1 - ss2 * sin2o;
+            const A r2 = -ss2 * cos2o1 - s1 * sin2o;
+            s0 += A(1.0) * r0; s1 += A(1.0) * r1; s2 += A(1.0) * r2; s3 += A(1.0) * A(0.0);
+            const A k2 = A(2.0) * mu * dt;
             s0 += k2 * e0; s1 += k2 * e1; s2 += k2 * e2; s3 += k2 * e3;
             ste2s = sqrt(second_inv(s0, s1, s2, s3));
             sta2s = sqrt(second_inv(e0, e1, e2, e3));
@@ -592,61 +602,61 @@ __global__ void SALEC_BOUNDS_STRESS k_stress(const CtxT<R> c)
     }
 
     if (state == 2) {
-        dam = 0.;
+        dam = A(0.);
     } else if (state == 1) {
-        dam = 1.0;
+        dam = A(1.0);
     } else {
-        double shear = 0.0, tensile = 0.;
+        A shear = A(0.0), tensile = A(0.);
         #pragma unroll
         for (int m = 1; m < nmat; ++m) {
-            const double vm = vmat[m];
-            if (vm < SALEC_TOLVOF) continue;
+            const A vm = vmat[m];
+            if (PLN(c.f.m_vof, m)[p] < SALEC_TOLVOF) continue;
             const DevMat &s = c.mat[m];
-            double my = strength_fn(s.yfunc, pre, dam, tps, sta2s, tem, 0., s);
-            if (c.rp.acoustic_fluid && pre >= 0.) {
-                const double vibp = dmin(rho * csd * sqrt(c.f.e_vib[p]), pre);
-                const double tm = simon_melt(pre, s);
-                double soft = ohnaka_soft(tem, s, tm);
-                soft = wind(soft, 0.0, 1.0);
-                const double lp = pre - vibp * dam * dam * sqrt(soft);
-                const double myv = strength_fn(s.yfunc, lp, dam, tps, sta2s, tem, 0., s) + rho * s.Acvis * sta2s;
-                my = dmin(myv, my);
+            A my = strength_fn<A>(s.yfunc, pre, dam, tps, sta2s, tem, A(0.), s);
+            if (c.rp.acoustic_fluid && pre >= A(0.)) {
+                const A vibp = amin(rho * csd * sqrt(A(c.f.e_vib[p])), pre);
+                const A tm = simon_melt<A>(pre, s);
+                A soft = ohnaka_soft<A>(tem, s, tm);
+                soft = awind(soft, A(0.0), A(1.0));
+                const A lp = pre - vibp * dam * dam * sqrt(soft);
+                const A myv = strength_fn<A>(s.yfunc, lp, dam, tps, sta2s, tem, A(0.), s) + rho * A(s.Acvis) * sta2s;
+                my = amin(myv, my);
             }
-            shear += vm * dmax(my, 0.0);
-            if (c.rp.tensile_failure) tensile += vm * strength_fn(s.tfunc, pre, dam, tps, sta2s, tem, 0., s);
+            shear += vm * amax(my, A(0.0));
+            if (c.rp.tensile_failure) tensile += vm * strength_fn<A>(s.tfunc, pre, dam, tps, sta2s, tem, A(0.), s);
         }
-        if (c.rp.tracer_lubrication >= 1 && c.f.e_cnd[p] >= 1.0) {
-            const double lub = dmin(pre * c.rp.tracer_lub_frac + c.rp.tracer_lub_y0, 0.0);
-            shear = dmin(shear, lub);
+        if (c.rp.tracer_lubrication >= 1 && c.f.e_cnd[p] >= A(1.0)) {
+            const A lub = amin(pre * A(c.rp.tracer_lub_frac) + A(c.rp.tracer_lub_y0), A(0.0));
+            shear = amin(shear, lub);
         }
         strength = shear;
         if (shear < ste2s) {
-            sta2s = sta2s / dmax(0.5, (ste2s - ste2s_old) / (ste2s - shear));
-            const double sfac = shear / ste2s;
+            sta2s = sta2s / amax(A(0.5), (ste2s - ste2s_old) / (ste2s - shear));
+            const A sfac = shear / ste2s;
             s0 *= sfac; s1 *= sfac; s2 *= sfac; s3 *= sfac;
             ste2s = shear;
-            double dsd = 0.;
+            A dsd = A(0.);
             #pragma unroll
             for (int m = 1; m < nmat; ++m) {
                 const DevMat &s = c.mat[m];
-                dsd += vmat[m] * strength_fn(s.dsdf, pre, dam, 0., 0., 0., 0., s);
+                dsd += vmat[m] * strength_fn<A>(s.dsdf, pre, dam, A(0.), A(0.), A(0.), A(0.), s);
             }
-            dam = wind(dam + sta2s * dsd * dt, 0.0, 1.0);
-            tps = dmin(tps + sta2s * dt, 10.);
+            dam = awind(dam + sta2s * dsd * dt, A(0.0), A(1.0));
+            tps = amin(tps + sta2s * dt, A(10.));
         }
         if (c.rp.tensile_failure) {
-            const double sxx = s0, szz = s2, sxz = s1, sth = s3;
-            const double ts = sqrt(sxz * sxz + 0.25 * (sxx - szz) * (sxx - szz));
-            double tmax = dmax(0.5 * (sxx + szz) - ts, 0.5 * (sxx + szz) + ts);
-            tmax = dmax(tmax, sth);
+            const A sxx = s0, szz = s2, sxz = s1, sth = s3;
+            const A ts = sqrt(sxz * sxz + A(0.25) * (sxx - szz) * (sxx - szz));
+            A tmax = amax(A(0.5) * (sxx + szz) - ts, A(0.5) * (sxx + szz) + ts);
+            tmax = amax(tmax, sth);
             if ((tmax - pre) > tensile) {
                 // the reference divides by Min(e_pos[1], e_pos[2]) (centre y and scale x)
-                const double dinc = 0.4 * csd / dmin(PLN(c.f.e_pos, 1)[p], PLN(c.f.e_pos, 2)[p]);
-                const double dold = dam;
-                double third = pow(dold, 1.0 / 3.);
+                const A dinc = A(0.4) * csd / A(dmin(PLN(c.f.e_pos, 1)[p], PLN(c.f.e_pos, 2)[p]));
+                const A dold = dam;
+                A third = pow(dold, A(1.0 / 3.));
                 third += dinc;
-                dam = wind(pow(third, 3.0), 0., 1.);
-                const double sfac = dold < 0.98 ? (1.0 - dam) / (1.0 - dold) : 0.0;
+                dam = awind(pow(third, A(3.0)), A(0.), A(1.));
+                const A sfac = dold < A(0.98) ? (A(1.0) - dam) / (A(1.0) - dold) : A(0.0);
                 s0 *= sfac; s1 *= sfac; s2 *= sfac; s3 *= sfac;
                 ste2s *= sfac;
             }
@@ -667,100 +677,104 @@ __global__ void SALEC_BOUNDS_STRESS k_stress(const CtxT<R> c)
 template <class R>
 __global__ void SALEC_BOUNDS_ACCEL k_vertex_acceleration(const CtxT<R> c)
 {
+    using A = R;   // arithmetic of the stress divergence: FP64, or FP32 in the mixed form
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!vert_active(c, i, j)) return;
     const long long p = KIDX(i, j);
     const long long cl[4] = {KIDX(i - 1, j - 1), KIDX(i, j - 1), KIDX(i, j), KIDX(i - 1, j)};
     const bool pml = (c.rp.damp_type == 1 || c.rp.damp_type == 2);
-    const double dt = c.scal->dt;
-    double ax = 0., ay = 0., vmass = 0., vvol = 0.;
-    double sub[4];
+    const A dt = A(c.scal->dt);
+    A ax = A(0.), ay = A(0.), vmass = A(0.), vvol = A(0.);
+    A sub[4];
     for (int k = 0; k < 4; ++k) sub[k] = GEO(c.g_v_subvol, k);
-    double sigx = 0., sigy = 0.;
-    double alx = 0., aly = 0.;
+    A sigx = A(0.), sigy = A(0.);
+    A alx = A(0.), aly = A(0.);
     if (pml) {
-        for (int k = 0; k < 4; ++k) { sigx += 0.25 * c.f.e_sigma[cl[k]]; sigy += 0.25 * PLN(c.f.e_sigma, 1)[cl[k]]; }
+        for (int k = 0; k < 4; ++k) {
+            sigx += A(0.25) * A(c.f.e_sigma[cl[k]]);
+            sigy += A(0.25) * A(PLN(c.f.e_sigma, 1)[cl[k]]);
+        }
         alx = c.f.v_alpha[p];
         aly = PLN(c.f.v_alpha, 1)[p];
     }
-    const bool damped = pml && (sigx > 0. || sigy > 0.);
+    const bool damped = pml && (sigx > A(0.) || sigy > A(0.));
     for (int k = 0; k < 4; ++k) {
         const long long e = cl[k];
-        const double sfx = GEO(c.g_v_suf, 2 * k), sfy = GEO(c.g_v_suf, 2 * k + 1);
-        const double lp = c.f.e_pre[e] + c.f.e_q[e];
-        const double ste0 = c.f.e_ste[e], ste1 = PLN(c.f.e_ste, 1)[e], ste2 = PLN(c.f.e_ste, 2)[e],
-                     ste3 = PLN(c.f.e_ste, 3)[e];
+        const A sfx = GEO(c.g_v_suf, 2 * k), sfy = GEO(c.g_v_suf, 2 * k + 1);
+        const A lp = A(c.f.e_pre[e]) + A(c.f.e_q[e]);
+        const A ste0 = c.f.e_ste[e], ste1 = PLN(c.f.e_ste, 1)[e], ste2 = PLN(c.f.e_ste, 2)[e],
+                ste3 = PLN(c.f.e_ste, 3)[e];
         if (!pml) {
-            double fpx = 0., fpy = 0.;
+            A fpx = A(0.), fpy = A(0.);
             fpx += lp * sfx;
             fpy += lp * sfy;
             fpx += sub[k] * lp;
-            const double sxx = ste0, szz = ste2, sxz = ste1, sth = ste3;
-            double fsx = 0., fsy = 0.;
+            const A sxx = ste0, szz = ste2, sxz = ste1, sth = ste3;
+            A fsx = A(0.), fsy = A(0.);
             fsx += sfx * sxx; fsx += sfy * sxz;
             fsy += sfx * sxz; fsy += sfy * szz;
             fsx += sub[k] * sth;
-            ax += -1.0 * fsx; ay += -1.0 * fsy;
-            ax += 1.0 * fpx; ay += 1.0 * fpy;
+            ax += A(-1.0) * fsx; ay += A(-1.0) * fsy;
+            ax += A(1.0) * fpx; ay += A(1.0) * fpy;
         } else {
-            const double lpr = PLN(c.f.e_dampref, 2)[e];
-            double sxx = ste0 - lp, szz = ste2 - lp, sxz = ste1, sth = ste3 - lp;
-            double fsx = 0., fsy = 0.;
+            const A lpr = PLN(c.f.e_dampref, 2)[e];
+            A sxx = ste0 - lp, szz = ste2 - lp, sxz = ste1, sth = ste3 - lp;
+            A fsx = A(0.), fsy = A(0.);
             fsx += sfx * sxx; fsx += sfy * sxz;
             fsy += sfx * sxz; fsy += sfy * szz;
             fsx += sub[k] * sth;
-            ax += -1.0 * fsx; ay += -1.0 * fsy;
+            ax += A(-1.0) * fsx; ay += A(-1.0) * fsy;
             if (damped) {
                 sxx += lpr; szz += lpr; sth += lpr;
-                double t0 = 0.; t0 += sfx * (sigy * sxx); t0 += sfy * (sigx * sxz);
+                A t0 = A(0.); t0 += sfx * (sigy * sxx); t0 += sfy * (sigx * sxz);
                 alx += t0 * dt;
-                double t1 = 0.; t1 += sfx * (sigy * sxz); t1 += sfy * (sigx * szz);
+                A t1 = A(0.); t1 += sfx * (sigy * sxz); t1 += sfy * (sigx * szz);
                 aly += t1 * dt;
                 alx += (sigx + sigy) * sub[k] * sth * dt;
             }
         }
-        const double lv = GEO(c.g_v_vol, 1 + k);
-        vmass += lv * c.f.e_den[e];
+        const A lv = GEO(c.g_v_vol, 1 + k);
+        vmass += lv * A(c.f.e_den[e]);
         vvol += lv;
     }
     if (damped) {
-        alx -= c.rp.alpha_damp_x * alx * dt;
-        aly -= c.rp.alpha_damp_y * aly * dt;
-        ax += -1.0 * alx; ay += -1.0 * aly;
+        alx -= A(c.rp.alpha_damp_x) * alx * dt;
+        aly -= A(c.rp.alpha_damp_y) * aly * dt;
+        ax += A(-1.0) * alx; ay += A(-1.0) * aly;
     }
     if (pml) { c.f.v_alpha[p] = alx; PLN(c.f.v_alpha, 1)[p] = aly; }
 
-    double ancx = 0., ancy = 0.;
+    A ancx = A(0.), ancy = A(0.);
     // where all nine weights are zero (outside the ANC band) the stencil sums to +0 and the term
     // is +0: the weights are not read there
     const bool lap = (c.lap_mask[(long long)j * (c.d.P >> 5) + (i >> 5)] >> (i & 31)) & 1u;
     if (!vert_pad(c, i, j) && lap) {
-        double lvx = 0., lvy = 0.;
+        A lvx = A(0.), lvy = A(0.);
         int k = 0;
         for (int dj = -1; dj <= 1; ++dj)
             for (int di = -1; di <= 1; ++di, ++k) {
                 const long long q = KIDX(i + di, j + dj);
-                const double w = PLN(c.f.v_laplace, k)[p];
-                lvx += w * c.f.v_vel[q];
-                lvy += w * PLN(c.f.v_vel, 1)[q];
+                const A w = PLN(c.f.v_laplace, k)[p];
+                lvx += w * A(c.f.v_vel[q]);
+                lvy += w * A(PLN(c.f.v_vel, 1)[q]);
             }
-        const double sc = 5.0e3 * sqrt(fabs(sub[0]) + fabs(sub[2]));
+        const A sc = A(5.0e3) * sqrt(fabs(sub[0]) + fabs(sub[2]));
         ancx = sc * lvx;
         ancy = sc * lvy;
     }
-    if (PLN(c.f.v_mass, 1)[p] >= 1.) { ancx = 0.; ancy = 0.; }
-    if (vmass > SALEC_TOLRHO * vvol) {
-        const double s = 1.0 / vmass;
+    if (PLN(c.f.v_mass, 1)[p] >= A(1.)) { ancx = A(0.); ancy = A(0.); }
+    if (vmass > A(SALEC_TOLRHO) * vvol) {
+        const A s = A(1.0) / vmass;
         ax *= s; ay *= s;
-        ax += 1.0 * c.f.v_bf[p]; ay += 1.0 * PLN(c.f.v_bf, 1)[p];
-        ax += c.rp.anc * ancx; ay += c.rp.anc * ancy;
+        ax += A(1.0) * A(c.f.v_bf[p]); ay += A(1.0) * A(PLN(c.f.v_bf, 1)[p]);
+        ax += A(c.rp.anc) * ancx; ay += A(c.rp.anc) * ancy;
     } else if (pml) {
         ax = c.f.v_bf[p]; ay = PLN(c.f.v_bf, 1)[p];
     } else {
-        ax = 0.; ay = 0.;
+        ax = A(0.); ay = A(0.);
     }
-    if (fabs(ax) < c.rp.acceleration_min * 1) ax = 0.;
-    if (fabs(ay) < c.rp.acceleration_min * 1) ay = 0.;
+    if (fabs(ax) < A(c.rp.acceleration_min * 1)) ax = A(0.);
+    if (fabs(ay) < A(c.rp.acceleration_min * 1)) ay = A(0.);
     c.f.v_acc[p] = ax;
     PLN(c.f.v_acc, 1)[p] = ay;
 }
@@ -947,84 +961,6 @@ __global__ void k_strength_condition(const CtxT<R> c)
 // A face with zero swept volume gets zero material volumes, which stands in for the
 // reference's clean_flux (src/advect.c:597-626): the other members of such a record are only
 // ever multiplied by those zero volumes.
-__device__ __forceinline__ double swept_volume(double xa, double ya, double xb, double yb, double dxa,
-                                               double dya, double dxb, double dyb)
-{
-    // get_flux_volcyl (src/advect.c:1347-1354)
-    const double x1 = -1.0 * dxa, y1 = -1.0 * dya, x2 = -1.0 * dxb, y2 = -1.0 * dyb;
-    const double vol = x1 * (ya - yb - y2) + x2 * (ya - yb + y1) + (y1 + y2) * (xb - xa);
-    return vol * fabs(2.0 * xa + 2.0 * xb + x1 + x2) / 8.0;
-}
-
-__device__ __forceinline__ double face_ratio(double p1, double p2)
-{
-    // geometric_flux_ratio (src/advect.c:1312-1330)
-    double a = p1, b = p2;
-    if (b > a) { a = p2; b = p1; }
-    if (b >= 0.0) return 1.0;
-    if (a <= 0.0) return 0.0;
-    return a / (a + fabs(b));
-}
-
-__device__ __forceinline__ double cut_length(double vf, double a, double b)
-{
-    // cut_length / cut_length_l / cut_length_s (src/advect.c:1356-1407)
-    if (a < b) { double t = a; a = b; b = t; }
-    if (1.0e-5 * a > b) {
-        double d;
-        if (vf <= 0.0) d = 0.0;
-        else if (vf <= 1.0) d = vf * a;
-        else d = a;
-        return d + b;
-    }
-    const double crf1 = 0.5 * b / a;
-    if (vf <= crf1) return sqrt(2.0 * a * b * vf);
-    if (vf <= 1.0 - crf1) return 0.5 * b + a * vf;
-    if (vf <= 1.0) return a + b - sqrt(2.0 * a * b * (1.0 - vf));
-    return a + b;
-}
-
-__device__ __forceinline__ void normalise2(double &x, double &y)
-{
-    // vec_norm (src/geometry/linear.c:132-146)
-    double len = 0.;
-    len += x * x;
-    len += y * y;
-    len = sqrt(len);
-    x /= len;
-    if (isnan(x)) x = 1.0;
-    y /= len;
-    if (isnan(y)) y = 1.0;
-}
-
-__device__ __forceinline__ double mstacs(double nd, double gf, double cr)
-{
-    // vofMSTACS (src/advect.c:1259-1274)
-    double cds, st;
-    if (cr < 1.0 / 3.0) cds = dmin(nd / cr, 1.0);
-    else cds = dmin(3.0 * nd, 1.0);
-    if (nd < 1.0 / 5.0) st = 3.0 * nd;
-    else if (nd < 1.0 / 2.0) st = (1.0 + nd) / 2.0;
-    else st = dmin((6.0 * nd + 3.0) / 8.0, 1.0);
-    return gf * cds + (1.0 - gf) * st;
-}
-
-__device__ __forceinline__ double algebraic_ratio(double vu, double vd, double va, double cr, double nx, double ny,
-                                                  double gx, double gy)
-{
-    // algebraic_flux_ratio (src/advect.c:1226-1253)
-    const double tmp = va - vu;
-    const double nd = (vd - vu) / tmp;
-    if (fabs(tmp) < SALEC_TOLVOF) return vd;
-    if (nd < SALEC_TOLVOF || nd > 1.0 - SALEC_TOLVOF) return vd;
-    double dot = 0.; dot += gx * nx; dot += gy * ny;
-    double len = 0.; len += gx * gx; len += gy * gy;
-    double cost = dot / sqrt(len);
-    cost = cost * cost;
-    const double gf = dmin(SALEC_CISSAMK1 * cost * cost, 1.0);
-    return vu + mstacs(nd, gf, cr) * (va - vu);
-}
-
 // Upwind record of one face of cell p (_calculate_flux_set_bphi, src/advect.c:1138-1223): the
 // face is written by the cell it flows out of; a face with zero swept volume gets zero material
 // volumes (see k_flux).
@@ -1687,44 +1623,45 @@ template <class R, int NM, bool POR>
 __device__ __forceinline__ void state_cell(const CtxT<R> &c, long long p, const CellState<NM, POR> &s)
 {
     constexpr int MM = CellState<NM, POR>::MM;
+    using A = R;   // arithmetic of the table interpolation and the mixture rules: FP64, or FP32 in the mixed form
     const int nmat = NM > 0 ? NM : c.d.nmat;
     constexpr bool por = POR;
     const double dam = s.dam;
-    double mpre[MM], mcsd[MM], mtem[MM];
-    double epre = 0.0, ecsd = 0.0, etem = 0.0, eden = 0.0, emu = 0.0;
+    A mpre[MM], mcsd[MM], mtem[MM];
+    A epre = A(0.0), ecsd = A(0.0), etem = A(0.0), eden = A(0.0), emu = A(0.0);
     #pragma unroll
     for (int m = 1; m < nmat; ++m) {
         const double vm = s.vof[m];
         if (vm < SALEC_TOLVOF) {
-            mpre[m] = 0.; mcsd[m] = 1.; mtem[m] = 0.;
+            mpre[m] = A(0.); mcsd[m] = A(1.); mtem[m] = A(0.);
         } else {
             const DevMat &ms = c.mat[m];
             const double plim = (1.0 - dam) * ms.minPint + dam * ms.minPdam;
             const double pt = por ? s.pty[m] : 1.0;
-            material_state(ms, s.rho[m], s.eng[m], plim, pt, mtem[m], mpre[m], mcsd[m]);
+            material_state<A>(ms, s.rho[m], s.eng[m], plim, pt, mtem[m], mpre[m], mcsd[m]);
         }
     }
     #pragma unroll
     for (int m = 1; m < nmat; ++m) {
-        const double vm = s.vof[m];
-        const double rm = s.rho[m];
+        const A vm = A(s.vof[m]);
+        const A rm = A(s.rho[m]);
         epre += vm * mpre[m];
-        ecsd += vm / dmax(1.0, mcsd[m]);
+        ecsd += vm / amax(A(1.0), mcsd[m]);
         etem += vm * mtem[m];
         eden += vm * rm;
-        emu += vm / dmax(1.0, rm * mcsd[m] * mcsd[m] * c.mat[m].GaCoef);
+        emu += vm / amax(A(1.0), rm * mcsd[m] * mcsd[m] * A(c.mat[m].GaCoef));
     }
-    if (emu > 0.) emu = 1.0 / emu;
-    if (ecsd > 0.) ecsd = 1.0 / ecsd;
+    if (emu > A(0.)) emu = A(1.0) / emu;
+    if (ecsd > A(0.)) ecsd = A(1.0) / ecsd;
     const double v0 = s.vof[0];
     if ((c.rp.partpres == 0 && v0 > SALEC_TOLVOF) || (c.rp.partpres == 1 && v0 > 1.0 - SALEC_TOLVOF)) {
-        epre = 0.;
-        ecsd = 1.0;
-        emu = 0.;
+        epre = A(0.);
+        ecsd = A(1.0);
+        emu = A(0.);
     } else if (c.rp.partpres == 1) {
-        ecsd = ecsd * (1.0 - v0);
-        etem = etem / (1.0 - v0);
-        emu = emu * (1.0 - v0);
+        ecsd = ecsd * A(1.0 - v0);
+        etem = etem / A(1.0 - v0);
+        emu = emu * A(1.0 - v0);
     }
     c.f.e_pre[p] = epre;
     c.f.e_csd[p] = ecsd;

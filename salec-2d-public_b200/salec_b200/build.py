@@ -16,8 +16,8 @@ ROOT = os.path.dirname(PKG)               # salec-2d-public_b200/
 CSRC = os.path.join(ROOT, "csrc")
 LIB = os.path.join(PKG, "libsalec_b200.so")
 SOURCES = ["salec_step.cu", "salec_runtime.cu", "salec_init.cu", "salec_noalloc.cu", "salec_output.cu",
-           "salec_ghost.cpp"]
-HEADERS = ["salec_device.cuh", "salec_kernels.h", "salec_deck.h"]
+           "salec_conserve.cu", "salec_adjoint.cu", "salec_ghost.cpp"]
+HEADERS = ["salec_device.cuh", "salec_kernels.h", "salec_deck.h", "salec_dual.cuh", "salec_adjoint.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "--fmad=false", "-lineinfo",
               "-std=c++17", "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-warn-spills"]
 

@@ -38,6 +38,10 @@ class RunDesc(ctypes.Structure):
                 ("tracer_lub_y0", c_d), ("tracer_lub_frac", c_d),
                 ("max_dt", c_d), ("dt", c_d), ("time", c_d), ("i_step", c_i), ("precision", c_i)]
 
+class AdjointResult(ctypes.Structure):
+    _fields_ = [("misfit", c_d), ("d_params", c_d * 4), ("d_velocity_scale", c_d)]
+
+
 PRECISION_FP64 = 0    # salec_precision: plain FP64 (bit-parity form)
 PRECISION_MIXED = 1   # FP32 storage of the relaxed fields, FP64 arithmetic and conserved fields
 
@@ -94,6 +98,14 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_set_tracers": ([vp, c_i, P_D], c_i),
             "salec_gpu_get_tracers": ([vp, P_D, ctypes.POINTER(c_i)], c_i),
             "salec_gpu_check": ([vp, ctypes.POINTER(c_ll)], c_i),
+            "salec_gpu_conservation": ([vp, P_D, c_i], c_i),
+            "salec_gpu_set_dt_schedule": ([vp, P_D, c_i], c_i),
+            "salec_gpu_adjoint_reset": ([vp], c_i),
+            "salec_gpu_adjoint_set_field": ([vp, c_i, P_D, c_ll], c_i),
+            "salec_gpu_adjoint_get_field": ([vp, c_i, P_D, c_ll], c_i),
+            "salec_gpu_adjoint_phase": ([vp, c_i], c_i),
+            "salec_gpu_adjoint_params": ([vp, P_D], c_i),
+            "salec_gpu_adjoint_window": ([vp, c_i, c_i, P_D, P_D, c_i, P_D, c_ll, ctypes.POINTER(AdjointResult)], c_i),
             "salec_gpu_write_output": ([vp, ctypes.c_char_p, ctypes.c_char_p, c_i, c_i, c_i], c_i),
             "salec_gpu_output_wait": ([vp], c_i),
             "salec_gpu_func_index": ([ctypes.c_char_p], c_i),
@@ -348,6 +360,55 @@ class Simulation:
         if code not in (SALEC_OK, -6):
             _check(code, "check")
         return n.value
+
+    def conservation(self) -> Dict[str, object]:
+        """Compensated FP64 conservation sums of the current state (salec_gpu_conservation):
+        total mass, r and z momentum, internal and kinetic energy, mass per material."""
+        nmat = self.get_run().nmat
+        out = np.zeros(4 + nmat)
+        _check(lib().salec_gpu_conservation(self.h, _ptr(out), len(out)), "salec_gpu_conservation")
+        return {"mass": float(out[0]), "momentum_r": float(out[1]), "momentum_z": float(out[2]),
+                "internal_energy": float(out[3]), "kinetic_energy": float(out[4]),
+                "mass_by_material": [float(x) for x in out[5:]]}
+
+    def set_dt_schedule(self, dts) -> None:
+        """Prescribed time steps for the next len(dts) cycles (salec_gpu_set_dt_schedule)."""
+        a = np.ascontiguousarray(dts, dtype=np.float64)
+        _check(lib().salec_gpu_set_dt_schedule(self.h, _ptr(a) if a.size else None, int(a.size)),
+               "salec_gpu_set_dt_schedule")
+
+    # ---- adjoint (salec_gpu_adjoint_*)
+    def adjoint_reset(self) -> None:
+        _check(lib().salec_gpu_adjoint_reset(self.h), "salec_gpu_adjoint_reset")
+
+    def adjoint_set(self, name: str, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        _check(lib().salec_gpu_adjoint_set_field(self.h, field_index(name), _ptr(a), a.size), "adjoint_set " + name)
+
+    def adjoint_get(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape(name), dtype=np.float64)
+        _check(lib().salec_gpu_adjoint_get_field(self.h, field_index(name), _ptr(out), out.size), "adjoint_get " + name)
+        return out
+
+    def adjoint_phase(self, phase: int) -> None:
+        _check(lib().salec_gpu_adjoint_phase(self.h, int(phase)), "salec_gpu_adjoint_phase")
+
+    def adjoint_params(self) -> np.ndarray:
+        out = np.zeros(4)
+        _check(lib().salec_gpu_adjoint_params(self.h, _ptr(out)), "salec_gpu_adjoint_params")
+        return out
+
+    def adjoint_window(self, nsteps: int, every: int, target, weight=None, density: bool = True):
+        """Adjoint of the next nsteps cycles (checkpoint every `every`) for the surface-height misfit
+        against target; returns (misfit, d_params[4], d_velocity_scale, grad_density or None)."""
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        w = None if weight is None else np.ascontiguousarray(weight, dtype=np.float64)
+        res = AdjointResult()
+        g = np.zeros(self.shape("e_den")[:2]) if density else None
+        _check(lib().salec_gpu_adjoint_window(self.h, int(nsteps), int(every), _ptr(t), None if w is None else _ptr(w),
+                                              t.size, None if g is None else _ptr(g), 0 if g is None else g.size,
+                                              ctypes.byref(res)), "salec_gpu_adjoint_window")
+        return res.misfit, np.array(res.d_params[:]), res.d_velocity_scale, g
 
     def set_tracers(self, rows: np.ndarray) -> None:
         r = np.ascontiguousarray(rows, dtype=np.float64).reshape(-1, 12)

@@ -134,6 +134,9 @@ class Deck:
     ejecta_friction: float = 0.0
     target_temperature: float = 293.0
     projectile_temperature: float = 293.0
+    # write every number with 17 significant digits (the exact double), e.g. for finite
+    # differences of a material parameter; False keeps the 6-digit form
+    exact: bool = False
     extra: Dict[str, Dict[str, str]] = dataclasses.field(default_factory=dict)
 
 
@@ -321,6 +324,7 @@ def write_deck(deck: Deck, folder: str, stem: str = "deck") -> str:
                 write_aneos_td(fn, m.name)
         else:
             raise ValueError("unsupported eos " + m.eos)
+    _g = (lambda v: "%.17g" % v) if deck.exact else globals()["_g"]
     radius = deck.radius_cells * deck.dy
     depth_total = deck.npy * deck.oy * deck.dy
     max_depth = deck.max_depth if deck.max_depth > 0 else 2.0 * depth_total
@@ -521,3 +525,28 @@ def ensemble_decks(count: int = 256, seed: int = 2024, nmin: int = 128, nmax: in
                         velocity=-v, gravity=-1.62, damping="pml", damp_x=damp, damp_y=damp, maxstep=1999,
                         dt0=1.0e-4, maxdt=0.05))
     return out
+
+
+def config5_deck(n: int = 512, cohesion: float = 1.0e7, friction: float = 1.2, velocity: float = 8000.0,
+                 cppr: float = 20.0, maxstep: int = 199) -> Deck:
+    """n x n cells at 50 m, basalt Tillotson target and projectile (CPPR 20, 8 km/s), the
+    Drucker-Prager parameters as RockStrengthT's intact and damaged cohesion (yint0 = ydam0),
+    friction (yintfri = ydamfri) and limit 2.5 GPa, Ivanov damage, gravity. The deck of the
+    adjoint window: no damping layers (the shock stays far from the boundaries over 200 cycles),
+    numbers written exactly so that finite differences of a parameter reach the solver."""
+    basalt = Material("basalt_", yint0=cohesion, yintfri=friction, yintlim=2.5e9, ydam0=cohesion,
+                      ydamfri=friction, ydamlim=2.5e9)
+    return Deck(npx=n, npy=n, dx=50.0, dy=50.0, oy=0.5, materials=[basalt], target_materials=["basalt_"],
+                target_depths=[1.0e7], projectile="basalt_", radius_cells=cppr, velocity=-velocity, gravity=-1.62,
+                damping="none", damp_x=0, damp_y=0, maxstep=maxstep, dt0=1.0e-4, maxdt=0.05, exact=True)
+
+
+def target_profile(h0: np.ndarray, dx: float, seed: int = 5) -> np.ndarray:
+    """Seeded target surface-height profile for the adjoint misfit: the initial material column
+    heights h0 (one per interior column) with a Gaussian bowl cut out (depth U[200, 400] m, width
+    U[20, 40] cells, centred on the axis) and +-1 m seeded roughness."""
+    rng = np.random.default_rng(seed)
+    depth = rng.uniform(200.0, 400.0)
+    width = rng.uniform(20.0, 40.0) * dx
+    r = (np.arange(len(h0)) + 0.5) * dx
+    return h0 - depth * np.exp(-(r / width) ** 2) + rng.uniform(-1.0, 1.0, len(h0))

@@ -1,0 +1,160 @@
+"""Adjoint of the mesh update against central finite differences (FP64, CUDA device).
+
+Per phase (dot-product test): from a developed state of the adjoint's deck, the reverse of phase
+p applied to random output adjoints ybar must satisfy <ybar, J dx> = <J^T ybar, dx> for a random
+relative perturbation dx of p's inputs, with J dx from central differences of the forward phase
+(relative step 1e-7). Tolerance: 1e-5 relative.
+
+Window: the adjoint of a checkpointed window against central differences (relative step 1e-6,
+frozen time steps, as the adjoint differentiates) of the surface-height misfit with respect to
+cohesion, friction, the initial velocity scale (impactor speed) and the initial density field
+along a random direction. Tolerance: 1e-3 relative.
+"""
+import numpy as np
+import pytest
+
+from salec_b200 import capi, decks
+
+# phase -> (input fields perturbed, output fields seeded)
+PHASE_IO = {
+    1: (["m_vof", "e_dvel", "e_den", "v_vel", "v_mass"], ["v_vof", "v_vel", "v_mass"]),
+    3: (["v_vel", "v_mass"], ["e_vel"]),
+    4: (["e_vel", "e_den"], ["v_vel"]),
+    5: (["v_vel", "e_den", "e_csd"], ["e_grad_vel", "e_div_vel", "e_q"]),
+    7: (["e_ste", "e_ste2s", "e_dam", "e_grad_vel", "e_mu", "e_pre", "e_tem", "m_vof"], ["e_ste", "e_ste2s", "e_dam"]),
+    8: (["e_pre", "e_q", "e_ste", "e_den", "v_vel"], ["v_acc"]),
+    9: (["v_vel", "v_acc"], ["v_dis", "v_vel"]),
+    10: (["e_pre", "e_q", "e_div_vel", "e_grad_vel", "e_ste", "m_eng"], ["m_eng"]),
+    12: (["v_dis", "m_vof", "v_vof", "m_den", "m_eng", "e_vel", "e_ste", "e_dam"], ["bx_phi", "by_phi"]),
+    14: (["bx_phi", "by_phi", "m_vof", "m_den", "m_eng", "e_den", "e_ste", "e_dam"],
+         ["m_vof", "m_den", "m_eng", "e_dvel", "e_ste", "e_dam", "e_den", "e_pre", "e_csd", "e_tem", "e_mu"]),
+}
+STATE = sorted({f for i, o in PHASE_IO.values() for f in i + o} | {"e_wpt", "v_acc", "v_dis"})
+EPS_PHASE = 1e-7
+TOL_PHASE = 1e-5
+EPS_FD = 1e-6
+TOL_FD = 1e-3
+
+
+def column_heights(sim):
+    vof, pos = sim.get_field("m_vof"), sim.get_field("e_pos")
+    return ((1.0 - vof[2:-2, 2:-2, 0]) * pos[2:-2, 2:-2, 3]).sum(axis=0)
+
+
+def misfit(sim, target):
+    r = column_heights(sim) - target
+    return 0.5 * float(np.sum(r * r))
+
+
+@pytest.fixture(scope="module")
+def developed(tmp_path_factory):
+    folder = str(tmp_path_factory.mktemp("adj"))
+    deck = decks.write_deck(decks.config5_deck(n=48, cppr=6.0), folder)
+    sim = capi.Simulation.from_deck(deck, folder)
+    sim.step(12)
+    state = {f: sim.get_field(f) for f in STATE}
+    dt = sim.scalar("dt")
+    return sim, state, dt
+
+
+def _set(sim, state, dt, delta=None, eps=0.0):
+    for f, a in state.items():
+        sim.set_field(f, a + eps * delta[f] if delta is not None and f in delta else a)
+    sim.set_scalar("dt", dt)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("phase", sorted(PHASE_IO))
+def test_adjoint_phase_dot_product(cuda_device, developed, phase):
+    sim, state, dt = developed
+    ins, outs = PHASE_IO[phase]
+    rng = np.random.default_rng(100 + phase)
+    delta = {f: state[f] * rng.uniform(-1.0, 1.0, state[f].shape) for f in ins}
+    if "v_mass" in delta:
+        delta["v_mass"][..., 1] = 0.0   # the void-corner count is an integer, not differentiated
+    ybar = {f: rng.uniform(-1.0, 1.0, state[f].shape) / max(float(np.sqrt(np.mean(state[f] ** 2))), 1e-30)
+            for f in outs}
+    res = {}
+    for sgn in (1.0, -1.0):
+        _set(sim, state, dt, delta, sgn * EPS_PHASE)
+        sim.phases(phase, phase)
+        res[sgn] = {f: sim.get_field(f) for f in outs}
+    lhs = sum(float(np.sum(ybar[f] * (res[1.0][f] - res[-1.0][f]))) for f in outs) / (2.0 * EPS_PHASE)
+    _set(sim, state, dt)
+    sim.adjoint_reset()
+    for f in outs:
+        sim.adjoint_set(f, ybar[f])
+    sim.adjoint_phase(phase)
+    terms = {f: float(np.sum(sim.adjoint_get(f) * delta[f])) for f in ins}
+    rhs = sum(terms.values())
+    scale = max(abs(lhs), abs(rhs), 1e-300)
+    assert abs(lhs - rhs) <= TOL_PHASE * scale, "phase %d: FD %.12e adjoint %.12e (terms %s)" % (phase, lhs, rhs, terms)
+
+
+def _fd_run(deck_kw, folder, dts, target, init_edit=None):
+    deck = decks.write_deck(decks.config5_deck(**deck_kw), folder)
+    sim = capi.Simulation.from_deck(deck, folder)
+    if init_edit:
+        init_edit(sim)
+    sim.set_dt_schedule(dts)
+    sim.step(len(dts))
+    J = misfit(sim, target)
+    sim.close()
+    return J
+
+
+@pytest.mark.gpu
+def test_adjoint_window_against_finite_differences(cuda_device, tmp_path):
+    base = dict(n=64, cppr=6.0, cohesion=1.0e7, friction=1.2, velocity=8000.0)
+    nsteps, every = 30, 10
+    folder = str(tmp_path / "base")
+    deck = decks.write_deck(decks.config5_deck(**base), folder)
+    ref = capi.Simulation.from_deck(deck, folder)
+    h0 = column_heights(ref)
+    target = decks.target_profile(h0, 50.0)
+    dts = []
+    for _ in range(nsteps):
+        ref.step(1)
+        dts.append(ref.scalar("dt"))
+    J_ref = misfit(ref, target)
+    ref.close()
+    sim = capi.Simulation.from_deck(deck, folder)
+    v0 = sim.get_field("v_vel")
+    md0, ed0 = sim.get_field("m_den"), sim.get_field("e_den")
+    J, dp, dvs, gden = sim.adjoint_window(nsteps, every, target)
+    assert abs(J - J_ref) <= 1e-12 * J_ref
+    sim.close()
+
+    def fd(kw_plus, kw_minus, edit_plus=None, edit_minus=None):
+        jp = _fd_run({**base, **kw_plus}, str(tmp_path / "p"), dts, target, edit_plus)
+        jm = _fd_run({**base, **kw_minus}, str(tmp_path / "m"), dts, target, edit_minus)
+        return jp - jm
+
+    c = base["cohesion"]
+    d_coh = fd({"cohesion": c * (1 + EPS_FD)}, {"cohesion": c * (1 - EPS_FD)}) / (2 * EPS_FD * c)
+    f = base["friction"]
+    d_fri = fd({"friction": f * (1 + EPS_FD)}, {"friction": f * (1 - EPS_FD)}) / (2 * EPS_FD * f)
+
+    def scale_v(s):
+        return lambda sim: sim.set_field("v_vel", v0 * s)
+
+    d_vel = fd({}, {}, scale_v(1 + EPS_FD), scale_v(1 - EPS_FD)) / (2 * EPS_FD)
+    rng = np.random.default_rng(7)
+    ds = rng.uniform(-1.0, 1.0, ed0.shape[:2])
+
+    def scale_rho(sg):
+        def edit(sim):
+            f_ = 1.0 + sg * EPS_FD * ds
+            md = md0.copy()
+            md[..., 1:] *= f_[..., None]
+            sim.set_field("m_den", md)
+            sim.set_field("e_den", ed0 * f_[..., None])
+        return edit
+
+    d_rho = fd({}, {}, scale_rho(1.0), scale_rho(-1.0)) / (2 * EPS_FD)
+    adj = {"cohesion": dp[0] + dp[2], "friction": dp[1] + dp[3], "velocity": dvs,
+           "density": float(np.sum(gden * ed0[..., 0] * ds))}
+    fds = {"cohesion": d_coh, "friction": d_fri, "velocity": d_vel, "density": d_rho}
+    print("adjoint", adj, "finite differences", fds)
+    for k in adj:
+        assert abs(adj[k] - fds[k]) <= TOL_FD * max(abs(fds[k]), 1e-300), (k, adj[k], fds[k])
