@@ -840,6 +840,123 @@ def run_ensemble(args):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- adjoint mode
+def column_heights(sim) -> np.ndarray:
+    vof, pos = sim.get_field("m_vof"), sim.get_field("e_pos")
+    return ((1.0 - vof[2:-2, 2:-2, 0]) * pos[2:-2, 2:-2, 3]).sum(axis=0)
+
+
+def run_adjoint(args):
+    """--adjoint: the adjoint of a window of --adj-steps cycles (checkpoint every --adj-every) on the
+    basalt deck of decks.config5_deck (n x n cells, CPPR 20, 8 km/s, Drucker-Prager as RockStrengthT
+    cohesion/friction, no damping layers), for the misfit of the final surface-height profile against
+    a seeded target. Times the forward window and the adjoint window with CUDA events on the
+    library's stream, and checks the cohesion, friction, impactor-speed and density gradients
+    against FP64 central finite differences (relative step 1e-6, frozen time steps)."""
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    ranks = Ranks("nccl")
+    n = args.adj_n
+    base = dict(n=n, cohesion=1.0e7, friction=1.2, velocity=8000.0, cppr=20.0)
+    tmp = tempfile.mkdtemp(prefix="salec_adj_%d_" % rank)
+    deck = decks.write_deck(decks.config5_deck(**base), tmp)
+    sim = capi.Simulation.from_deck(deck, tmp)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    h0 = column_heights(sim)
+    target = decks.target_profile(h0, 50.0)
+    v0, md0, ed0 = sim.get_field("v_vel"), sim.get_field("m_den"), sim.get_field("e_den")
+    init_state = snapshot(sim, torch)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    # forward window (warm-up first), recording the time steps
+    sim.step(args.warmup)
+    restore(sim, init_state)
+    sim.sync()
+    dts = []
+    ranks.barrier()
+    ev[0].record(stream)
+    for _ in range(args.adj_steps):
+        sim.step(1)
+    ev[1].record(stream)
+    ev[1].synchronize()
+    fwd_ms = ev[0].elapsed_time(ev[1])
+    restore(sim, init_state)
+    for _ in range(args.adj_steps):
+        sim.step(1)
+        dts.append(sim.scalar("dt"))
+    r = column_heights(sim) - target
+    J_fwd = 0.5 * float(np.sum(r * r))
+    # adjoint window (its own forward pass, replays and reverse sweeps), once untimed
+    restore(sim, init_state)
+    sim.adjoint_window(args.adj_steps, args.adj_every, target, density=False)
+    restore(sim, init_state)
+    sim.sync()
+    ranks.barrier()
+    ev[2].record(stream)
+    J, dp, dvs, gden = sim.adjoint_window(args.adj_steps, args.adj_every, target)
+    ev[3].record(stream)
+    ev[3].synchronize()
+    adj_ms = ev[2].elapsed_time(ev[3])
+    adj_ms_max, fwd_ms_max = ranks.all_max(adj_ms), ranks.all_max(fwd_ms)
+    sim.close()
+
+    def fd_run(kw, edit=None):
+        d = decks.write_deck(decks.config5_deck(**{**base, **kw}), os.path.join(tmp, "fd"))
+        s_ = capi.Simulation.from_deck(d, os.path.join(tmp, "fd"))
+        if edit:
+            edit(s_)
+        s_.set_dt_schedule(dts)
+        s_.step(len(dts))
+        rr = column_heights(s_) - target
+        s_.close()
+        return 0.5 * float(np.sum(rr * rr))
+
+    eps = 1e-6
+    fd = {}
+    c, f = base["cohesion"], base["friction"]
+    fd["cohesion"] = (fd_run({"cohesion": c * (1 + eps)}) - fd_run({"cohesion": c * (1 - eps)})) / (2 * eps * c)
+    fd["friction"] = (fd_run({"friction": f * (1 + eps)}) - fd_run({"friction": f * (1 - eps)})) / (2 * eps * f)
+    fd["speed"] = (fd_run({}, lambda s_: s_.set_field("v_vel", v0 * (1 + eps))) -
+                   fd_run({}, lambda s_: s_.set_field("v_vel", v0 * (1 - eps)))) / (2 * eps * base["velocity"])
+    rng = np.random.default_rng(11)
+    ds = rng.uniform(-1.0, 1.0, ed0.shape[:2])
+
+    def rho_edit(sg):
+        def e(s_):
+            fac = 1.0 + sg * eps * ds
+            md = md0.copy()
+            md[..., 1:] *= fac[..., None]
+            s_.set_field("m_den", md)
+            s_.set_field("e_den", ed0 * fac[..., None])
+        return e
+
+    fd["density_direction"] = (fd_run({}, rho_edit(1.0)) - fd_run({}, rho_edit(-1.0))) / (2 * eps)
+    adj = {"cohesion": float(dp[0] + dp[2]), "friction": float(dp[1] + dp[3]),
+           "speed": float(dvs / base["velocity"]), "density_direction": float(np.sum(gden * ed0[..., 0] * ds))}
+    rel = {k: abs(adj[k] - fd[k]) / max(abs(fd[k]), 1e-300) for k in adj}
+    ranks.close()
+    if rank == 0:
+        cells = n * n
+        print(json.dumps({
+            "metric": "adjoint/forward cost", "value": adj_ms_max / fwd_ms_max, "unit": "ratio", "n_gpus": world,
+            "steps": args.adj_steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "adjoint of %d cycles, %dx%d basalt, CPPR 20 at 8 km/s, Drucker-Prager as "
+                                   "RockStrengthT (cohesion 10 MPa, friction 1.2), no damping layers" % (args.adj_steps, n, n),
+                       "checkpoint_every": args.adj_every,
+                       "functional": "0.5 sum_i (h_i - target_i)^2, h_i the material column height of interior "
+                                     "column i at the window's end, seeded target (decks.target_profile)",
+                       "timing": "CUDA events on the library's stream: forward window of --adj-steps cycles vs "
+                                 "salec_gpu_adjoint_window (its forward pass, checkpoints, replays and reverse sweeps)"},
+            "forward_ms": fwd_ms_max, "adjoint_ms": adj_ms_max,
+            "forward_cell_updates_per_s": world * cells * args.adj_steps / (fwd_ms_max / 1000.0),
+            "misfit": J, "misfit_forward": J_fwd,
+            "gradients": {"adjoint": adj, "finite_difference": fd, "rel_err": rel,
+                          "fd_step": "1e-6 relative, central, frozen time steps",
+                          "d_params_raw": [float(x) for x in dp]},
+            "nonfinite_grad_density": int(np.count_nonzero(~np.isfinite(gden)))}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -855,7 +972,7 @@ def main():
                     help="cycles of the whole-run timing and of the mixed-vs-FP64 accuracy run at the configured "
                          "length (0: skip)")
     ap.add_argument("--chunk", type=int, default=250, help="cycles per timed chunk of the whole run")
-    ap.add_argument("--start-cycle", type=int, default=0,
+    ap.add_argument("--start-cycle", type=int, default=2500,
                     help="untimed cycles from the deck's initial state before the warm-up and timed window")
     ap.add_argument("--ensemble", type=int, default=0, help="run the ensemble mode with this many members")
     ap.add_argument("--ens-steps", type=int, default=2000)
@@ -867,13 +984,19 @@ def main():
     ap.add_argument("--layered", action="store_true",
                     help="run the layered three-material target (plain and mixed forms) instead")
     ap.add_argument("--layered-n", type=int, default=4096, help="cells per side of the layered target")
+    ap.add_argument("--adjoint", action="store_true", help="run the adjoint window (configuration 5) instead")
+    ap.add_argument("--adj-n", type=int, default=512, help="cells per side of the adjoint deck")
+    ap.add_argument("--adj-steps", type=int, default=200)
+    ap.add_argument("--adj-every", type=int, default=20)
     ap.add_argument("--block-shapes", default="",
                     help='JSON {phase: [x, y]} of block shapes to set instead of autotuning, '
                          'e.g. the "block_shapes_by_phase" of an earlier run')
     args = ap.parse_args()
     if args.warmup < 1:
         args.warmup = 1
-    if args.ensemble > 0 and args.impl == "ours":
+    if args.adjoint and args.impl == "ours":
+        run_adjoint(args)
+    elif args.ensemble > 0 and args.impl == "ours":
         run_ensemble(args)
     elif args.layered and args.impl == "ours":
         run_layered(args)

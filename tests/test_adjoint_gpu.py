@@ -30,7 +30,7 @@ PHASE_IO = {
          ["m_vof", "m_den", "m_eng", "e_dvel", "e_ste", "e_dam", "e_den", "e_pre", "e_csd", "e_tem", "e_mu"]),
 }
 STATE = sorted({f for i, o in PHASE_IO.values() for f in i + o} | {"e_wpt", "v_acc", "v_dis"})
-EPS_PHASE = 1e-7
+EPS_PHASE = 1e-8
 TOL_PHASE = 1e-5
 EPS_FD = 1e-6
 TOL_FD = 1e-3
@@ -49,7 +49,10 @@ def misfit(sim, target):
 @pytest.fixture(scope="module")
 def developed(tmp_path_factory):
     folder = str(tmp_path_factory.mktemp("adj"))
-    deck = decks.write_deck(decks.config5_deck(n=48, cppr=6.0), folder)
+    # a 1 km/s impact: plastic flow and damage growth without vaporisation, so that few points sit
+    # on a kink of the forward model (clamps, min/max switches), where central differences average
+    # the two one-sided derivatives
+    deck = decks.write_deck(decks.config5_deck(n=48, cppr=6.0, velocity=1000.0), folder)
     sim = capi.Simulation.from_deck(deck, folder)
     sim.step(12)
     state = {f: sim.get_field(f) for f in STATE}
@@ -66,6 +69,7 @@ def _set(sim, state, dt, delta=None, eps=0.0):
 @pytest.mark.gpu
 @pytest.mark.parametrize("phase", sorted(PHASE_IO))
 def test_adjoint_phase_dot_product(cuda_device, developed, phase):
+    """One input field at a time: <ybar, J_f dx_f> from central differences against <xbar_f, dx_f>."""
     sim, state, dt = developed
     ins, outs = PHASE_IO[phase]
     rng = np.random.default_rng(100 + phase)
@@ -74,21 +78,32 @@ def test_adjoint_phase_dot_product(cuda_device, developed, phase):
         delta["v_mass"][..., 1] = 0.0   # the void-corner count is an integer, not differentiated
     ybar = {f: rng.uniform(-1.0, 1.0, state[f].shape) / max(float(np.sqrt(np.mean(state[f] ** 2))), 1e-30)
             for f in outs}
-    res = {}
-    for sgn in (1.0, -1.0):
-        _set(sim, state, dt, delta, sgn * EPS_PHASE)
-        sim.phases(phase, phase)
-        res[sgn] = {f: sim.get_field(f) for f in outs}
-    lhs = sum(float(np.sum(ybar[f] * (res[1.0][f] - res[-1.0][f]))) for f in outs) / (2.0 * EPS_PHASE)
+    if phase == 5:
+        # the viscosity switches on where the velocity divergence turns negative; inside a uniformly
+        # moving body the divergence is zero up to rounding, a kink that any perturbation crosses
+        _set(sim, state, dt)
+        sim.phases(5, 5)
+        div = sim.get_field("e_div_vel")
+        ybar["e_q"][np.abs(div) < 1e-6 * float(np.max(np.abs(div)))] = 0.0
     _set(sim, state, dt)
     sim.adjoint_reset()
     for f in outs:
         sim.adjoint_set(f, ybar[f])
     sim.adjoint_phase(phase)
-    terms = {f: float(np.sum(sim.adjoint_get(f) * delta[f])) for f in ins}
-    rhs = sum(terms.values())
-    scale = max(abs(lhs), abs(rhs), 1e-300)
-    assert abs(lhs - rhs) <= TOL_PHASE * scale, "phase %d: FD %.12e adjoint %.12e (terms %s)" % (phase, lhs, rhs, terms)
+    rhs = {f: float(np.sum(sim.adjoint_get(f) * delta[f])) for f in ins}
+    lhs = {}
+    for f in ins:
+        res = {}
+        for sgn in (1.0, -1.0):
+            _set(sim, state, dt, {f: delta[f]}, sgn * EPS_PHASE)
+            sim.phases(phase, phase)
+            res[sgn] = {o: sim.get_field(o) for o in outs}
+        lhs[f] = sum(float(np.sum(ybar[o] * (res[1.0][o] - res[-1.0][o]))) for o in outs) / (2.0 * EPS_PHASE)
+    _set(sim, state, dt)
+    bad = {f: (lhs[f], rhs[f]) for f in ins
+           if abs(lhs[f] - rhs[f]) > TOL_PHASE * max(abs(lhs[f]), abs(rhs[f]), 1e-300)}
+    print("phase", phase, {f: "%.9e / %.9e" % (lhs[f], rhs[f]) for f in ins})
+    assert not bad, "phase %d: finite differences vs adjoint per input field %s" % (phase, bad)
 
 
 def _fd_run(deck_kw, folder, dts, target, init_edit=None):
@@ -105,7 +120,7 @@ def _fd_run(deck_kw, folder, dts, target, init_edit=None):
 
 @pytest.mark.gpu
 def test_adjoint_window_against_finite_differences(cuda_device, tmp_path):
-    base = dict(n=64, cppr=6.0, cohesion=1.0e7, friction=1.2, velocity=8000.0)
+    base = dict(n=64, cppr=6.0, cohesion=1.0e7, friction=1.2, velocity=1000.0)
     nsteps, every = 30, 10
     folder = str(tmp_path / "base")
     deck = decks.write_deck(decks.config5_deck(**base), folder)
