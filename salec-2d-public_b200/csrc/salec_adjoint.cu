@@ -254,6 +254,12 @@ __global__ void ka_gradient(const AdjCtx a)
         for (int k = 0; k < 4; ++k) d3 += g[4 + k] * vy[k];
         for (int k = 0; k < 4; ++k) d4 += g[8 + k] * vx[k];
         const double div = d0 + d3 + d4;
+        // a divergence that is zero to within the rounding of its terms (a body at rest or in
+        // uniform motion) sits on the kink of the viscosity, min(0, div) below the TOLQPRE cut:
+        // the derivative there is the average of the two sides, -rho ql / 2 and 0
+        double dterms = 0.;
+        for (int k = 0; k < 4; ++k) dterms += fabs(g[k] * vx[k]) + fabs(g[4 + k] * vy[k]) + fabs(g[8 + k] * vx[k]);
+        const bool on_kink = fabs(div) <= 1e-12 * dterms;
         const double vof0 = c.f.m_vof[p];
         if (!(vof0 > SALEC_TOLVOF || c.f.e_pre[p] <= 0.0)) {
             double area = GEO(c.g_e_vol, 0) / c.f.e_pos[p];
@@ -262,7 +268,9 @@ __global__ void ka_gradient(const AdjCtx a)
             const double ql = c.rp.avis1 * csd * sqrt(area);
             const double qq = c.rp.avis2 * div * area;
             const double q = dmin(0., div) * rho * (qq - ql);
-            if (!(q < SALEC_TOLQPRE) && div < 0.) {
+            if (on_kink) {
+                gdiv += gq * (-0.5 * rho * ql);
+            } else if (!(q < SALEC_TOLQPRE) && div < 0.) {
                 gdiv += gq * (rho * (qq - ql) + div * rho * c.rp.avis2 * area);
                 a.b.e_den[p] += gq * div * (qq - ql);
                 a.b.e_csd[p] += gq * (-div * rho * c.rp.avis1 * sqrt(area));
@@ -661,15 +669,24 @@ __global__ void ka_flux(const AdjCtx a)
         for (int k = 0; k < 4; ++k) gx += vq[k] * grd[k];
         for (int k = 0; k < 4; ++k) gy += vq[k] * grd[4 + k];
         normalise2(gx, gy);
+        // a cut line parallel to a mesh line up to the rounding of the fraction gradient (a
+        // component of about 1e-16) sits on the kinks of |n| and of the corner maximum, which a
+        // perturbation of the fractions crosses: it is put on them, so that the derivatives are
+        // the averages of both sides
+        snap_zero(gx, 1e-12);
+        snap_zero(gy, 1e-12);
         D ca = PLN(c.f.e_pos, 2)[p] * fabs(gx);
         D cb = PLN(c.f.e_pos, 3)[p] * fabs(gy);
         if (ca < cb) { D t = ca; ca = cb; cb = t; }
         const D dstar = cut_length(vpd, ca, cb);
         D lw[4];
         for (int k = 0; k < 4; ++k) { D s(0.); s += gx * px[k]; s += gy * py[k]; lw[k] = s; }
-        D mw = lw[0];
-        for (int k = 1; k < 4; ++k) if (lw[k] > mw) mw = lw[k];
-        // dmax(dmax(l0, l1), dmax(l2, l3)) picks, on ties, the same value
+        // dmax(dmax(l0, l1), dmax(l2, l3)) as the step forms it; ties (a horizontal or vertical cut
+        // line has two equal corners), to rounding, take the average of the one-sided derivatives
+        double lmax = 0.;
+        for (int k = 0; k < 4; ++k) lmax = dmax(lmax, fabs(lw[k].v));
+        const double ltol = 1e-12 * lmax;
+        const D mw = fmax_near(fmax_near(lw[0], lw[1], ltol), fmax_near(lw[2], lw[3], ltol), ltol);
         for (int k = 0; k < 4; ++k) lw[k] = lw[k] - mw + dstar;
         fpd[0] = face_ratio(lw[3], lw[0]);
         fpd[2] = face_ratio(lw[2], lw[1]);

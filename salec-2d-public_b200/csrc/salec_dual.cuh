@@ -119,7 +119,12 @@ template <int N> __host__ __device__ __forceinline__ Dual<N> tanh(const Dual<N> 
     const double t = ::tanh(a.v);
     return scale(a, 1.0 - t * t, t);
 }
-template <int N> __host__ __device__ __forceinline__ Dual<N> fabs(const Dual<N> &a) { return scale(a, a.v < 0.0 ? -1.0 : 1.0, ::fabs(a.v)); }
+// At a kink (|x| at 0, ties of min/max) the derivative is the average of the two one-sided
+// ones: what a symmetric (central) perturbation of the input sees.
+template <int N> __host__ __device__ __forceinline__ Dual<N> fabs(const Dual<N> &a)
+{
+    return scale(a, a.v < 0.0 ? -1.0 : (a.v > 0.0 ? 1.0 : 0.0), ::fabs(a.v));
+}
 template <int N> __host__ __device__ __forceinline__ Dual<N> pow(const Dual<N> &a, const Dual<N> &b)
 {
     // a^b = exp(b log a), for a > 0; the forward formulas raise positive bases only
@@ -131,8 +136,33 @@ template <int N> __host__ __device__ __forceinline__ Dual<N> pow(const Dual<N> &
     for (int k = 0; k < N; ++k) r.d[k] = da * a.d[k] + db * b.d[k];
     return r;
 }
-template <int N> __host__ __device__ __forceinline__ Dual<N> fmax(const Dual<N> &a, const Dual<N> &b) { return a.v >= b.v ? a : b; }
-template <int N> __host__ __device__ __forceinline__ Dual<N> fmin(const Dual<N> &a, const Dual<N> &b) { return a.v <= b.v ? a : b; }
+template <int N> __host__ __device__ __forceinline__ Dual<N> tie(const Dual<N> &a, const Dual<N> &b)
+{
+    return lin(a, 0.5, b, 0.5, a.v);
+}
+template <int N> __host__ __device__ __forceinline__ Dual<N> fmax(const Dual<N> &a, const Dual<N> &b)
+{
+    return a.v > b.v ? a : (b.v > a.v ? b : tie(a, b));
+}
+template <int N> __host__ __device__ __forceinline__ Dual<N> fmin(const Dual<N> &a, const Dual<N> &b)
+{
+    return a.v < b.v ? a : (b.v < a.v ? b : tie(a, b));
+}
+// max of two values that may differ by rounding only: within tol of each other they are a tie
+template <int N> __host__ __device__ __forceinline__ Dual<N> fmax_near(const Dual<N> &a, const Dual<N> &b, double tol)
+{
+    if (::fabs(a.v - b.v) > tol) return a.v > b.v ? a : b;
+    return lin(a, 0.5, b, 0.5, a.v > b.v ? a.v : b.v);
+}
+// a value within tol of zero, a kink of the formulas downstream (|x|, a corner maximum), is put on
+// the kink; its derivatives are kept
+template <int N> __host__ __device__ __forceinline__ void snap_zero(Dual<N> &a, double tol)
+{
+    if (::fabs(a.v) <= tol) a.v = 0.0;
+}
+// the min/max/clamp of the step's templated formulas, with the same tie rule
+template <int N> __host__ __device__ __forceinline__ Dual<N> amin(Dual<N> a, Dual<N> b) { return fmin(a, b); }
+template <int N> __host__ __device__ __forceinline__ Dual<N> amax(Dual<N> a, Dual<N> b) { return fmax(a, b); }
 template <int N> __host__ __device__ __forceinline__ Dual<N> floor(const Dual<N> &a) { return Dual<N>(::floor(a.v)); }
 template <int N> __host__ __device__ __forceinline__ double val(const Dual<N> &a) { return a.v; }
 

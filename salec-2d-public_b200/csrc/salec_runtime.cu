@@ -1450,6 +1450,10 @@ const std::vector<const char *> kAdjWrites[16] = {
     {},
 };
 
+// face flux records written by phase 12 and read by phase 14 and its reverse (the face normals
+// are fixed at start-up)
+const std::vector<const char *> kAdjFaces = {"bx_phi", "by_phi"};
+
 size_t field_bytes(const salec_gpu *h, int k)
 {
     const size_t col = (((size_t)h->d.enx + 31) / 32) * 32;
@@ -1756,6 +1760,10 @@ int salec_gpu_adjoint_window(salec_gpu *h, int nsteps, int every, const double *
     size_t ub = 0;
     std::vector<size_t> uoff(16);
     for (int p = 0; p < 16; ++p) { uoff[p] = ub; ub += list_bytes(h, kAdjWrites[p]); }
+    // the face flux records phase 12 leaves for phase 14 are kept per replayed cycle: the
+    // reverse of cycle k reads cycle k's, not the last replayed cycle's
+    const size_t fo = ub;
+    ub += list_bytes(h, kAdjFaces);
     // buffers: nseg + 1 checkpoints (the last is the window's end), `every` undo logs
     const size_t need_ck = sb * (nseg + 1), need_ud = ub * every;
     if (st->ckpt_bytes < need_ck) {
@@ -1818,12 +1826,18 @@ int salec_gpu_adjoint_window(salec_gpu *h, int nsteps, int every, const double *
             for (int p = 0; p <= 15; ++p) {
                 if (int rc = copy_list(h, kAdjWrites[p], log + uoff[p], true)) return rc;
                 if (int rc = run_phase(h, p)) return rc;
+                if (p == 12)
+                    if (int rc = copy_list(h, kAdjFaces, log + fo, true)) return rc;
             }
         }
         for (int k = n - 1; k >= 0; --k) {
             char *log = st->undo + ub * k;
             const double dt = dts[sgm * every + k];
             for (int p = 15; p >= 0; --p) {
+                // the faces first: their copy carries the scalars after phase 12, which the
+                // undo log of phase 14 then sets back to those before phase 14
+                if (p == 14)
+                    if (int rc = copy_list(h, kAdjFaces, log + fo, false)) return rc;
                 if (int rc = copy_list(h, kAdjWrites[p], log + uoff[p], false)) return rc;
                 if (int rc = adjoint_phase(h, p, dt)) return rc;
             }

@@ -134,6 +134,7 @@ class Deck:
     ejecta_friction: float = 0.0
     target_temperature: float = 293.0
     projectile_temperature: float = 293.0
+    projectile_pressure: float = 1.0e-5
     # write every number with 17 significant digits (the exact double), e.g. for finite
     # differences of a material parameter; False keeps the 6-digit form
     exact: bool = False
@@ -360,7 +361,7 @@ def write_deck(deck: Deck, folder: str, stem: str = "deck") -> str:
     w("    center = [%s, %s]" % (_g(0.0), _g(radius)))
     w("    velocity = [%s, %s]" % (_g(deck.vx), _g(deck.velocity)))
     w("    damage = [const, 0.0]")
-    w("    pressure = [const, 1.0e-5]")
+    w("    pressure = [const, %s]" % ("1.0e-5" if deck.projectile_pressure == 1.0e-5 else _g(deck.projectile_pressure)))
     w("    temperature = [const, %s]" % _g(deck.projectile_temperature))
     w("[target]")
     w("    type = plane")
@@ -533,12 +534,16 @@ def config5_deck(n: int = 512, cohesion: float = 1.0e7, friction: float = 1.2, v
     Drucker-Prager parameters as RockStrengthT's intact and damaged cohesion (yint0 = ydam0),
     friction (yintfri = ydamfri) and limit 2.5 GPa, Ivanov damage, gravity. The deck of the
     adjoint window: no damping layers (the shock stays far from the boundaries over 200 cycles),
-    numbers written exactly so that finite differences of a parameter reach the solver."""
+    numbers written exactly so that finite differences of a parameter reach the solver. The
+    projectile starts at 1 MPa: at the default 1e-5 Pa its cells sit exactly at rho0 with a
+    pressure below 0.01 Pa, on a node of the Tillotson cold-energy table and on the sound-speed
+    switch of the EOS, kinks where the derivative is one-sided."""
     basalt = Material("basalt_", yint0=cohesion, yintfri=friction, yintlim=2.5e9, ydam0=cohesion,
                       ydamfri=friction, ydamlim=2.5e9)
     return Deck(npx=n, npy=n, dx=50.0, dy=50.0, oy=0.5, materials=[basalt], target_materials=["basalt_"],
                 target_depths=[1.0e7], projectile="basalt_", radius_cells=cppr, velocity=-velocity, gravity=-1.62,
-                damping="none", damp_x=0, damp_y=0, maxstep=maxstep, dt0=1.0e-4, maxdt=0.05, exact=True)
+                damping="none", damp_x=0, damp_y=0, maxstep=maxstep, dt0=1.0e-4, maxdt=0.05, exact=True,
+                projectile_pressure=1.0e6)
 
 
 def target_profile(h0: np.ndarray, dx: float, seed: int = 5) -> np.ndarray:
