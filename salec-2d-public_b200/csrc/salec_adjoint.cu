@@ -296,7 +296,7 @@ __global__ void ka_stress(const AdjCtx a)
     double th[4] = {0., 0., 0., 0.};
     if (a_cell_interior(c, i, j)) {
         const long long p = KIDX(i, j);
-        const double dt = a.dt;
+        const double dt = c.scal->dt;
         const double vof0 = c.f.m_vof[p];
         if (vof0 > SALEC_TOLVOF) {
             for (int q = 0; q < 4; ++q) PLN(a.b.e_ste, q)[p] = 0.0;
@@ -537,7 +537,7 @@ __global__ void ka_displacement(const AdjCtx a)
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (!a_vert_active(c, i, j)) return;
     const long long p = KIDX(i, j);
-    const double dt = a.dt, hdt2 = 0.5 * dt * dt;
+    const double dt = c.scal->dt, hdt2 = 0.5 * dt * dt;
     for (int k = 0; k < 2; ++k) {
         const double gdis = PLN(a.b.v_dis, k)[p], gvel = PLN(a.b.v_vel, k)[p];
         PLN(a.b.v_vel, k)[p] = gvel + dt * gdis;
@@ -558,7 +558,7 @@ __global__ void ka_energy(const AdjCtx a)
     const double vm = PLN(c.f.m_vof, 1)[p], rm = PLN(c.f.m_den, 1)[p], em = PLN(c.f.m_eng, 1)[p];
     const double ge = PLN(a.b.m_eng, 1)[p];
     if (vm <= SALEC_TOLVOF || rm <= SALEC_TOLRHO) { PLN(a.b.m_eng, 1)[p] = 0.0; return; }
-    const double dt = a.dt;
+    const double dt = c.scal->dt;
     const double pre = c.f.e_pre[p], q = c.f.e_q[p], div = c.f.e_div_vel[p];
     double g[5], s[4];
     for (int k = 0; k < 5; ++k) g[k] = PLN(c.f.e_grad_vel, k)[p];
@@ -1122,7 +1122,39 @@ __global__ void ka_profile_seed(const Ctx c, const Fields b, const double *h, co
     if (j == 2) atomicAdd(J, 0.5 * w[col] * r * r);
 }
 
+__global__ void ka_list_copy(const CopySeg *segs, int nseg, char *base, const long long *slot,
+                             unsigned long long stride, int save)
+{
+    char *rec = base + (slot ? (unsigned long long)*slot * stride : 0ULL);
+    const unsigned long long t0 = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned long long nt = (unsigned long long)gridDim.x * blockDim.x;
+    for (int k = 0; k < nseg; ++k) {
+        const CopySeg g = segs[k];
+        char *dst = save ? rec + g.off : g.field;
+        const char *src = save ? g.field : rec + g.off;
+        const unsigned long long n16 = g.bytes >> 4;
+        for (unsigned long long q = t0; q < n16; q += nt)
+            reinterpret_cast<uint4 *>(dst)[q] = reinterpret_cast<const uint4 *>(src)[q];
+        for (unsigned long long q = (n16 << 4) + t0; q < g.bytes; q += nt) dst[q] = src[q];
+    }
+}
+
+__global__ void ka_slot(long long *slot, long long v, int add)
+{
+    if (threadIdx.x == 0) *slot = add ? *slot + v : v;
+}
+
 } // namespace
+
+void launch_list_copy(const CopySeg *segs, int nseg, char *base, const long long *slot, unsigned long long stride,
+                      bool save, cudaStream_t s)
+{
+    ka_list_copy<<<4 * 148, 256, 0, s>>>(segs, nseg, base, slot, stride, save ? 1 : 0);
+}
+
+void launch_slot_set(long long *slot, long long value, cudaStream_t s) { ka_slot<<<1, 32, 0, s>>>(slot, value, 0); }
+
+void launch_slot_add(long long *slot, long long delta, cudaStream_t s) { ka_slot<<<1, 32, 0, s>>>(slot, delta, 1); }
 
 void launch_adjoint_kernel(AdjKernel k, const AdjCtx &a, cudaStream_t s)
 {

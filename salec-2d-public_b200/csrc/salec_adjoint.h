@@ -6,14 +6,19 @@
 
 namespace salec {
 
-// Forward state before the sweep (c), adjoint planes in the same layout (b), the step's time
-// step, and the accumulators of the parameter gradients: theta[0] d/d cohesion (Yint0 = Ydam0),
-// theta[1] d/d friction (Yfricint = Yfricdam).
+// Forward state before the sweep (c; its scalar block holds the cycle's time step), adjoint
+// planes in the same layout (b), and the accumulators of the parameter gradients: d/d Yint0,
+// Yfricint, Ydam0, Yfricdam of material 1.
 struct AdjCtx {
     Ctx c;
     Fields b;
-    double dt;
     double *theta;
+};
+
+// One field of a list copy: its bytes at `field` and their place `off` in a log record.
+struct CopySeg {
+    char *field;
+    unsigned long long off, bytes;
 };
 
 // Reverse sweeps, numbered by the forward phase whose kernel they reverse.
@@ -32,6 +37,14 @@ void launch_adjoint_gather(const GatherBatch &g, const int *entries, const void 
 // over the interior rows; J = 0.5 * sum_i w_i (h_i - target_i)^2 (target and weights per
 // interior column); the adjoint of m_vof[0] receives -w_i (h_i - target_i) e_pos[3] and
 // *J (one double on the device) the misfit.
+// Copies a list of fields into (save) or out of a log record at base + slot * stride (slot read on
+// the device, so that one captured graph walks the records of a segment; a null slot is record
+// 0). Fields and record offsets are 16-byte aligned.
+void launch_list_copy(const CopySeg *segs, int nseg, char *base, const long long *slot, unsigned long long stride,
+                      bool save, cudaStream_t s);
+// *slot = value, or *slot += delta
+void launch_slot_set(long long *slot, long long value, cudaStream_t s);
+void launch_slot_add(long long *slot, long long delta, cudaStream_t s);
 void launch_profile_misfit(const Ctx &c, const Fields &b, const double *target, const double *weight, double *J,
                            double *h, cudaStream_t s);
 #endif

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -700,6 +701,7 @@ int transfer(salec_gpu *h, int fid, double *host, long long n, bool to_device)
 }
 
 void adjoint_release(salec_gpu *h);
+void adjoint_drop_graphs(salec_gpu *h);
 
 void release(salec_gpu *h)
 {
@@ -1014,6 +1016,7 @@ void drop_cycle_graph(salec_gpu *h)
 {
     if (h->cycle_graph) cudaGraphExecDestroy(h->cycle_graph);
     h->cycle_graph = nullptr;
+    adjoint_drop_graphs(h);
 }
 
 // Capture phases 0-15 of one cycle on the handle's stream into a graph; on any failure the
@@ -1417,6 +1420,15 @@ struct AdjointState {
     size_t undo_bytes = 0;
     double *mis = nullptr;         // misfit: J, column heights, target, weights
     size_t mis_doubles = 0;
+    struct ListCopy {
+        CopySeg *dev = nullptr;
+        int n = 0;
+    };
+    std::map<std::string, ListCopy> lists;   // device tables of the field lists copied to logs
+    long long *slot = nullptr;     // undo-log record of the cycle being replayed or reversed
+    cudaGraphExec_t replay = nullptr, reverse = nullptr;   // one replayed / one reversed cycle
+    const char *graph_undo = nullptr;   // undo buffer and record size the graphs were captured for
+    size_t graph_ub = 0;
 };
 
 namespace {
@@ -1468,28 +1480,72 @@ size_t list_bytes(const salec_gpu *h, const List &names)
     return (b + 255) & ~(size_t)255;
 }
 
-// copy the listed fields and the scalar block to (save) or from (restore) buf
-template <class List>
-int copy_list(salec_gpu *h, const List &names, char *buf, bool save)
+// fields the reverse recipes keep aside while they re-run a forward sub-step
+const std::vector<const char *> kKeep12 = {"m_den", "e_vib", "m_eng"};
+const std::vector<const char *> kKeep9 = {"v_dis", "v_vel"};
+const std::vector<const char *> kKeep8 = {"e_pre", "e_ste", "e_q", "v_acc"};
+const std::vector<const char *> kKeep3 = {"e_vel"};
+const std::vector<const char *> kKeep1 = {"m_vof", "e_dvel", "e_den", "v_vof", "v_vel", "v_mass"};
+
+// Device table of a field list: the fields in order, then the scalar block, at the offsets of
+// list_bytes' record layout. Built outside stream capture (adjoint_tables builds every list).
+const AdjointState::ListCopy *list_table(salec_gpu *h, const std::vector<const char *> &names)
 {
-    size_t off = 0;
+    AdjointState *st = h->adj;
+    std::string key;
+    for (const char *n : names) { key += n; key += ','; }
+    auto it = st->lists.find(key);
+    if (it != st->lists.end()) return &it->second;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(h->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return nullptr;
+    std::vector<CopySeg> segs;
+    unsigned long long off = 0;
     for (const char *n : names) {
         const int k = field_by_name(n);
         const size_t nb = field_bytes(h, k);
-        char *f = reinterpret_cast<char *>(field_ptr(h, k));
-        CUDA_TRY(cudaMemcpyAsync(save ? buf + off : f, save ? f : buf + off, nb, cudaMemcpyDeviceToDevice, h->stream));
+        segs.push_back({reinterpret_cast<char *>(field_ptr(h, k)), off, nb});
         off += nb;
     }
-    CUDA_TRY(cudaMemcpyAsync(save ? buf + off : reinterpret_cast<char *>(h->scal),
-                             save ? reinterpret_cast<char *>(h->scal) : buf + off, sizeof(Scal),
-                             cudaMemcpyDeviceToDevice, h->stream));
+    segs.push_back({reinterpret_cast<char *>(h->scal), off, sizeof(Scal)});
+    AdjointState::ListCopy L;
+    if (cudaMalloc(reinterpret_cast<void **>(&L.dev), segs.size() * sizeof(CopySeg)) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(L.dev, segs.data(), segs.size() * sizeof(CopySeg), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(L.dev);
+        return nullptr;
+    }
+    L.n = (int)segs.size();
+    return &(st->lists[key] = L);
+}
+
+// copy the listed fields and the scalar block to (save) or from (restore) the record at buf, or,
+// with slot, at buf + *slot * stride
+int copy_list(salec_gpu *h, const std::vector<const char *> &names, char *buf, bool save, const long long *slot = nullptr,
+              size_t stride = 0)
+{
+    const AdjointState::ListCopy *L = list_table(h, names);
+    if (!L) return fail(SALEC_ERR_CUDA, "adjoint: list table unavailable");
+    launch_list_copy(L->dev, L->n, buf, slot, stride, save, h->stream);
+    CUDA_TRY(cudaGetLastError());
     return SALEC_OK;
+}
+
+void adjoint_drop_graphs(salec_gpu *h)
+{
+    AdjointState *st = h->adj;
+    if (!st) return;
+    if (st->replay) cudaGraphExecDestroy(st->replay);
+    if (st->reverse) cudaGraphExecDestroy(st->reverse);
+    st->replay = st->reverse = nullptr;
+    st->graph_undo = nullptr;
 }
 
 void adjoint_release(salec_gpu *h)
 {
     AdjointState *st = h->adj;
     if (!st) return;
+    adjoint_drop_graphs(h);
+    for (auto &kv : st->lists) cudaFree(kv.second.dev);
+    cudaFree(st->slot);
     cudaFree(st->pool);
     cudaFree(st->theta);
     cudaFree(st->gscratch);
@@ -1542,6 +1598,14 @@ int adjoint_ensure(salec_gpu *h)
         for (int p = 0; p < 16; ++p) tb = std::max(tb, list_bytes(h, kAdjWrites[p]));
         st->tmp_bytes = tb;
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->tmp), tb));
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->slot), sizeof(long long)));
+        // every list table, so that the graphs can be captured
+        const std::vector<const char *> snap(std::begin(kAdjSnapshot), std::end(kAdjSnapshot));
+        std::vector<const std::vector<const char *> *> all = {&snap, &kAdjFaces, &kKeep12, &kKeep9, &kKeep8, &kKeep3,
+                                                              &kKeep1};
+        for (int p = 0; p < 16; ++p) all.push_back(&kAdjWrites[p]);
+        for (const auto *l : all)
+            if (!list_table(h, *l)) return fail(SALEC_ERR_CUDA, "adjoint: list table");
     }
     return SALEC_OK;
 }
@@ -1565,58 +1629,55 @@ int adjoint_gather(salec_gpu *h, const Gather &g)
 }
 
 // Reverse of phase p with the current field pool as the state before phase p (left so on return).
-int adjoint_phase(salec_gpu *h, int p, double dt)
+int adjoint_phase(salec_gpu *h, int p)
 {
     AdjointState *st = h->adj;
     AdjCtx a;
     a.c = h->ctx();
     a.b = st->b;
-    a.dt = dt;
     a.theta = st->theta;
     cudaStream_t s = h->stream;
     const Ctx &c = a.c;
-    auto keep = [&](std::initializer_list<const char *> names, bool save) {
-        return copy_list(h, std::vector<const char *>(names), st->tmp, save);
-    };
+    auto keep = [&](const std::vector<const char *> &names, bool save) { return copy_list(h, names, st->tmp, save); };
     int rc = SALEC_OK;
     switch (p) {
     case 14: launch_adjoint_kernel(AK_REMAP_STATE, a, s); break;
     case 12:
-        if ((rc = keep({"m_den", "e_vib", "m_eng"}, true))) return rc;
+        if ((rc = keep(kKeep12, true))) return rc;
         if ((rc = run_gather(h, h->g_flux_state))) return rc;
         launch_adjoint_kernel(AK_FLUX, a, s);
-        if ((rc = keep({"m_den", "e_vib", "m_eng"}, false))) return rc;
+        if ((rc = keep(kKeep12, false))) return rc;
         if ((rc = adjoint_gather(h, h->g_flux_state))) return rc;
         break;
     case 10: launch_adjoint_kernel(AK_ENERGY, a, s); break;
     case 9:
-        if ((rc = keep({"v_dis", "v_vel"}, true))) return rc;
+        if ((rc = keep(kKeep9, true))) return rc;
         launch_step_kernel(SK_DISPLACEMENT, c, s, h->blk[SK_DISPLACEMENT]);
         if ((rc = adjoint_gather(h, h->r_dis))) return rc;
-        if ((rc = keep({"v_dis", "v_vel"}, false))) return rc;
+        if ((rc = keep(kKeep9, false))) return rc;
         launch_adjoint_kernel(AK_DISPLACEMENT, a, s);
         break;
     case 8:
-        if ((rc = keep({"e_pre", "e_ste", "e_q", "v_acc"}, true))) return rc;
+        if ((rc = keep(kKeep8, true))) return rc;
         if ((rc = run_gather(h, h->g_pre_ste_q))) return rc;
         launch_step_kernel(SK_ACCELERATION, c, s, h->blk[SK_ACCELERATION]);
         if ((rc = adjoint_gather(h, h->r_acc))) return rc;
         launch_adjoint_kernel(AK_ACCELERATION, a, s);
-        if ((rc = keep({"e_pre", "e_ste", "e_q", "v_acc"}, false))) return rc;
+        if ((rc = keep(kKeep8, false))) return rc;
         if ((rc = adjoint_gather(h, h->g_pre_ste_q))) return rc;
         break;
     case 7: launch_adjoint_kernel(AK_STRESS, a, s); break;
     case 5: launch_adjoint_kernel(AK_GRADIENT, a, s); break;
     case 4: launch_adjoint_kernel(AK_VOID_VERTICES, a, s); break;
     case 3:
-        if ((rc = keep({"e_vel"}, true))) return rc;
+        if ((rc = keep(kKeep3, true))) return rc;
         launch_step_kernel(SK_CELL_VELOCITY, c, s, h->blk[SK_CELL_VELOCITY]);
         if ((rc = adjoint_gather(h, h->g_evel))) return rc;
-        if ((rc = keep({"e_vel"}, false))) return rc;
+        if ((rc = keep(kKeep3, false))) return rc;
         launch_adjoint_kernel(AK_CELL_VELOCITY, a, s);
         break;
     case 1: {
-        if ((rc = keep({"m_vof", "e_dvel", "e_den", "v_vof", "v_vel", "v_mass"}, true))) return rc;
+        if ((rc = keep(kKeep1, true))) return rc;
         if ((rc = run_gather(h, h->g_mvof))) return rc;
         if ((rc = run_gather(h, h->g_dvel_den))) return rc;
         launch_step_kernel(SK_VERTEX_VOF_MOMENTUM, c, s, h->blk[SK_VERTEX_VOF_MOMENTUM]);
@@ -1631,7 +1692,7 @@ int adjoint_phase(salec_gpu *h, int p, double dt)
             off += nb;
         }
         launch_adjoint_kernel(AK_VERTEX_MOMENTUM, a, s);
-        if ((rc = keep({"m_vof", "e_dvel", "e_den", "v_vof", "v_vel", "v_mass"}, false))) return rc;
+        if ((rc = keep(kKeep1, false))) return rc;
         if ((rc = adjoint_gather(h, h->g_dvel_den))) return rc;
         if ((rc = adjoint_gather(h, h->g_mvof))) return rc;
         break;
@@ -1670,6 +1731,66 @@ int adjoint_transfer(salec_gpu *h, int fid, double *host, long long n, bool to_d
     }
     slot = saved;
     return rc;
+}
+
+// Capture `body` on the handle's stream into an executable graph.
+int capture_graph(salec_gpu *h, const std::function<int()> &body, cudaGraphExec_t *exec)
+{
+    const long long before = h->launches;
+    CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = body();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    h->launches = before;
+    if (rc != SALEC_OK || e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return rc != SALEC_OK ? rc : fail(SALEC_ERR_CUDA, std::string("adjoint graph capture: ") + cudaGetErrorString(e));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return fail(SALEC_ERR_CUDA, std::string("adjoint graph: ") + cudaGetErrorString(ei));
+    return SALEC_OK;
+}
+
+// The two graphs of the window: one cycle replayed with its undo log written to record *slot,
+// and one cycle reversed from record *slot; each moves *slot on by one.
+int adjoint_graphs(salec_gpu *h, size_t ub, const std::vector<size_t> &uoff, size_t fo)
+{
+    AdjointState *st = h->adj;
+    if (st->replay && st->reverse && st->graph_undo == st->undo && st->graph_ub == ub) return SALEC_OK;
+    adjoint_drop_graphs(h);
+    cudaStream_t s = h->stream;
+    int rc = capture_graph(h, [&]() {
+        for (int p = 0; p <= 15; ++p) {
+            if (int r = copy_list(h, kAdjWrites[p], st->undo + uoff[p], true, st->slot, ub)) return r;
+            if (int r = run_phase(h, p)) return r;
+            if (p == 12)
+                if (int r = copy_list(h, kAdjFaces, st->undo + fo, true, st->slot, ub)) return r;
+        }
+        launch_slot_add(st->slot, 1, s);
+        return SALEC_OK;
+    }, &st->replay);
+    if (rc) return rc;
+    rc = capture_graph(h, [&]() {
+        for (int p = 15; p >= 0; --p) {
+            // the faces first: their record carries the scalars after phase 12, which the undo
+            // log of phase 14 then sets back to those before phase 14
+            if (p == 14)
+                if (int r = copy_list(h, kAdjFaces, st->undo + fo, false, st->slot, ub)) return r;
+            if (int r = copy_list(h, kAdjWrites[p], st->undo + uoff[p], false, st->slot, ub)) return r;
+            if (int r = adjoint_phase(h, p)) return r;
+        }
+        launch_slot_add(st->slot, -1, s);
+        return SALEC_OK;
+    }, &st->reverse);
+    if (rc) {
+        adjoint_drop_graphs(h);
+        return rc;
+    }
+    st->graph_undo = st->undo;
+    st->graph_ub = ub;
+    return SALEC_OK;
 }
 
 int adjoint_check(salec_gpu *h)
@@ -1730,8 +1851,7 @@ int salec_gpu_adjoint_phase(salec_gpu *h, int phase)
 {
     if (!h || !h->adj || !h->adj->pool) return fail(SALEC_ERR_STATE, "call salec_gpu_adjoint_reset first");
     if (phase < 0 || phase > 15) return fail(SALEC_ERR_ARG, "phase out of range");
-    CUDA_TRY(cudaMemcpy(h->scal_host, h->scal, sizeof(Scal), cudaMemcpyDeviceToHost));
-    if (int rc = adjoint_phase(h, phase, h->scal_host->dt)) return rc;
+    if (int rc = adjoint_phase(h, phase)) return rc;
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return SALEC_OK;
 }
@@ -1787,14 +1907,17 @@ int salec_gpu_adjoint_window(salec_gpu *h, int nsteps, int every, const double *
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->mis), md * sizeof(double)));
         st->mis_doubles = md;
     }
-    std::vector<double> dts(nsteps);
-    // forward window, with a checkpoint at every segment start
+    if (int rc = adjoint_graphs(h, ub, uoff, fo)) return rc;
+    // forward window, with a checkpoint at every segment start; the last segment writes its undo
+    // logs on the way, so that it is reversed without a replay
     for (int sgm = 0; sgm < nseg; ++sgm) {
         if (int rc = copy_list(h, snap, st->ckpt + sb * sgm, true)) return rc;
         const int n = std::min(every, nsteps - sgm * every);
-        for (int k = 0; k < n; ++k) {
-            if (int rc = salec_gpu_step(h, 1)) return rc;
-            CUDA_TRY(cudaMemcpyAsync(&dts[sgm * every + k], &h->scal->dt, sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (sgm < nseg - 1) {
+            if (int rc = salec_gpu_step(h, n)) return rc;
+        } else {
+            launch_slot_set(st->slot, 0, s);
+            for (int k = 0; k < n; ++k) CUDA_TRY(cudaGraphLaunch(st->replay, s));
         }
     }
     if (int rc = copy_list(h, snap, st->ckpt + sb * nseg, true)) return rc;
@@ -1819,29 +1942,14 @@ int salec_gpu_adjoint_window(salec_gpu *h, int nsteps, int every, const double *
     CUDA_TRY(cudaStreamSynchronize(s));
     // reverse: per segment, replay its cycles from the checkpoint with undo logs, then walk back
     for (int sgm = nseg - 1; sgm >= 0; --sgm) {
-        if (int rc = copy_list(h, snap, st->ckpt + sb * sgm, false)) return rc;
         const int n = std::min(every, nsteps - sgm * every);
-        for (int k = 0; k < n; ++k) {
-            char *log = st->undo + ub * k;
-            for (int p = 0; p <= 15; ++p) {
-                if (int rc = copy_list(h, kAdjWrites[p], log + uoff[p], true)) return rc;
-                if (int rc = run_phase(h, p)) return rc;
-                if (p == 12)
-                    if (int rc = copy_list(h, kAdjFaces, log + fo, true)) return rc;
-            }
+        if (sgm < nseg - 1) {
+            if (int rc = copy_list(h, snap, st->ckpt + sb * sgm, false)) return rc;
+            launch_slot_set(st->slot, 0, s);
+            for (int k = 0; k < n; ++k) CUDA_TRY(cudaGraphLaunch(st->replay, s));
         }
-        for (int k = n - 1; k >= 0; --k) {
-            char *log = st->undo + ub * k;
-            const double dt = dts[sgm * every + k];
-            for (int p = 15; p >= 0; --p) {
-                // the faces first: their copy carries the scalars after phase 12, which the
-                // undo log of phase 14 then sets back to those before phase 14
-                if (p == 14)
-                    if (int rc = copy_list(h, kAdjFaces, log + fo, false)) return rc;
-                if (int rc = copy_list(h, kAdjWrites[p], log + uoff[p], false)) return rc;
-                if (int rc = adjoint_phase(h, p, dt)) return rc;
-            }
-        }
+        launch_slot_set(st->slot, n - 1, s);
+        for (int k = 0; k < n; ++k) CUDA_TRY(cudaGraphLaunch(st->reverse, s));
     }
     // the pool now holds the window's start and the adjoint planes its sensitivities
     out->misfit = J;
