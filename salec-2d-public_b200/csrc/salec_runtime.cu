@@ -1761,7 +1761,7 @@ int adjoint_graphs(salec_gpu *h, size_t ub, const std::vector<size_t> &uoff, siz
     if (st->replay && st->reverse && st->graph_undo == st->undo && st->graph_ub == ub) return SALEC_OK;
     adjoint_drop_graphs(h);
     cudaStream_t s = h->stream;
-    int rc = capture_graph(h, [&]() {
+    int rc = capture_graph(h, [&]() -> int {
         for (int p = 0; p <= 15; ++p) {
             if (int r = copy_list(h, kAdjWrites[p], st->undo + uoff[p], true, st->slot, ub)) return r;
             if (int r = run_phase(h, p)) return r;
@@ -1772,7 +1772,7 @@ int adjoint_graphs(salec_gpu *h, size_t ub, const std::vector<size_t> &uoff, siz
         return SALEC_OK;
     }, &st->replay);
     if (rc) return rc;
-    rc = capture_graph(h, [&]() {
+    rc = capture_graph(h, [&]() -> int {
         for (int p = 15; p >= 0; --p) {
             // the faces first: their record carries the scalars after phase 12, which the undo
             // log of phase 14 then sets back to those before phase 14

@@ -77,6 +77,10 @@ def lib() -> ctypes.CDLL:
             except Exception as e:  # no nvcc on this machine: only a prebuilt library can be used
                 if not os.path.exists(path):
                     raise RuntimeError("libsalec_b200.so is missing and cannot be built: %s" % e)
+                # the prebuilt library is older than the sources: say so, it may not match them
+                import warnings
+                warnings.warn("libsalec_b200.so is older than its sources and the rebuild failed; "
+                              "using the prebuilt library: %s" % str(e)[-400:], RuntimeWarning)
         L = ctypes.CDLL(path)
         vp = ctypes.c_void_p
         sig = {
