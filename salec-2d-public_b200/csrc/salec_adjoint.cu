@@ -232,11 +232,9 @@ __global__ void ka_void_vertices(const AdjCtx a)
 
 // ---------------------------------------------------------------- phase 5: gradient, viscosity
 // update_e_gradvel with the artificial viscosity (src/sale2d.c:1144-1236)
-__global__ void ka_gradient(const AdjCtx a)
+__device__ __forceinline__ void gradient_adj(const AdjCtx &a, int i, int j, double corner[8])
 {
     const Ctx &c = a.c;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (!a_cell_interior(c, i, j)) return;
     const long long p = KIDX(i, j);
     double gd[5];
     for (int k = 0; k < 5; ++k) { gd[k] = PLN(a.b.e_grad_vel, k)[p]; PLN(a.b.e_grad_vel, k)[p] = 0.0; }
@@ -281,8 +279,43 @@ __global__ void ka_gradient(const AdjCtx a)
     gd[3] += gdiv;
     gd[4] += gdiv;
     for (int k = 0; k < 4; ++k) {
-        add(a.b.v_vel + vl[k], g[k] * gd[0] + g[4 + k] * gd[1] + g[8 + k] * gd[4]);
-        add(PLN(a.b.v_vel, 1) + vl[k], g[k] * gd[2] + g[4 + k] * gd[3]);
+        corner[2 * k] = g[k] * gd[0] + g[4 + k] * gd[1] + g[8 + k] * gd[4];
+        corner[2 * k + 1] = g[k] * gd[2] + g[4 + k] * gd[3];
+    }
+}
+
+// the vertex-velocity adjoints go to the corner scratch of the cell (planes 2k, 2k+1 for corner
+// k); ka_corner_sum adds them up per vertex, without atomics
+__global__ void ka_gradient(const AdjCtx a)
+{
+    const Ctx &c = a.c;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= c.d.enx || j >= c.d.eny) return;
+    double corner[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
+    if (a_cell_interior(c, i, j)) gradient_adj(a, i, j, corner);
+    const long long p = KIDX(i, j);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a.scr[q * c.d.PL + p] = corner[q];
+}
+
+// vertex (I, J) is corner 0 of cell (I, J), 1 of (I-1, J), 2 of (I-1, J-1), 3 of (I, J-1): the
+// sum of their corner scratch (planes first + 2k + comp) is added to dst's two components
+__global__ void ka_corner_sum(const AdjCtx a, double *dst, int first)
+{
+    const Ctx &c = a.c;
+    const int I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+    if (I >= c.d.vnx || J >= c.d.vny) return;
+    const long long PL = c.d.PL;
+    const bool in_x = I < c.d.enx, in_y = J < c.d.eny, lo_x = I >= 1, lo_y = J >= 1;
+#pragma unroll
+    for (int comp = 0; comp < 2; ++comp) {
+        const double *s = a.scr + (long long)(first + comp) * PL;
+        double v = 0.;
+        if (in_x && in_y) v += s[KIDX(I, J)];
+        if (lo_x && in_y) v += s[2 * PL + KIDX(I - 1, J)];
+        if (lo_x && lo_y) v += s[4 * PL + KIDX(I - 1, J - 1)];
+        if (in_x && lo_y) v += s[6 * PL + KIDX(I, J - 1)];
+        if (v != 0.0) dst[comp * PL + KIDX(I, J)] += v;
     }
 }
 
@@ -593,12 +626,20 @@ __device__ __forceinline__ void swept_volume_adj(double xa, double ya, double xb
     for (int k = 0; k < 4; ++k) out[k] = g * v.d[k];
 }
 
-__global__ void ka_flux(const AdjCtx a)
+// corner[2k + comp]: adjoint of v_dis at corner k; corner[8 + 2k + m]: adjoint of v_vof[m] there.
+// CUT selects the cells with a cut line (primary fraction below 1 - TOLVOF); the others take the
+// light instance, which holds none of the cut line's registers.
+template <bool CUT>
+__device__ __forceinline__ void flux_adj(const AdjCtx &a, int i, int j, double corner[16])
 {
     const Ctx &c = a.c;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= c.d.enx || j >= c.d.eny) return;
     const long long p = KIDX(i, j);
+    double vof[2] = {c.f.m_vof[p], PLN(c.f.m_vof, 1)[p]};
+    int prim = 0;
+    double vprim = vof[0];
+    if (vof[0] < SALEC_TOLVOF && vof[1] > vprim) { prim = 1; vprim = vof[1]; }
+    const bool full = vprim > 1.0 - SALEC_TOLVOF;
+    if (full == CUT) return;
     const long long vl[4] = {KIDX(i, j), KIDX(i + 1, j), KIDX(i + 1, j + 1), KIDX(i, j + 1)};
     double px[4], py[4], dx[4], dy[4];
     for (int k = 0; k < 4; ++k) {
@@ -616,45 +657,60 @@ __global__ void ka_flux(const AdjCtx a)
     const int nmat = 2;
     // adjoints of the records this cell writes (donor faces); the copied state members go to
     // the cell's own state
-    double gflux[2][4] = {{0., 0., 0., 0.}, {0., 0., 0., 0.}};
+    // adjoints of the material volumes of the records this cell writes (donor faces), by material;
+    // the copied state members go to the cell's own state
+    double g0[4] = {0., 0., 0., 0.}, g1[4] = {0., 0., 0., 0.};
     bool any = false;
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
-        if (vol[k] > 0.) continue;
-        double *f = bface[k];
-        for (int m = 0; m < nmat; ++m) { gflux[m][k] = f[m * PL]; f[m * PL] = 0.0; }
-        if (vol[k] == 0.) continue;
-        for (int m = 0; m < nmat; ++m) {
-            const double gr = f[(m + nmat) * PL], gen = f[(m + 2 * nmat) * PL];
-            f[(m + nmat) * PL] = 0.0;
-            f[(m + 2 * nmat) * PL] = 0.0;
-            if (gr != 0.0) PLN(a.b.m_den, m)[p] += gr;
-            if (gen != 0.0) PLN(a.b.m_eng, m)[p] += gen;
+        if (vol[k] <= 0.) {
+            double *f = bface[k];
+            g0[k] = f[0];
+            g1[k] = f[PL];
+            f[0] = 0.0;
+            f[PL] = 0.0;
+            if (vol[k] < 0.) {
+#pragma unroll
+                for (int m = 0; m < nmat; ++m) {
+                    const double gr = f[(m + nmat) * PL], gen = f[(m + 2 * nmat) * PL];
+                    f[(m + nmat) * PL] = 0.0;
+                    f[(m + 2 * nmat) * PL] = 0.0;
+                    if (gr != 0.0) PLN(a.b.m_den, m)[p] += gr;
+                    if (gen != 0.0) PLN(a.b.m_eng, m)[p] += gen;
+                }
+                const int b = 3 * nmat;
+                a.b.e_vel[p] += f[(b + 0) * PL];
+                PLN(a.b.e_vel, 1)[p] += f[(b + 1) * PL];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) PLN(a.b.e_ste, q)[p] += f[(b + 2 + q) * PL];
+                a.b.e_dam[p] += f[(b + 6) * PL];
+#pragma unroll
+                for (int q = 0; q < 10; ++q) f[(b + q) * PL] = 0.0;
+                any = true;
+            }
         }
-        const int b = 3 * nmat;
-        a.b.e_vel[p] += f[(b + 0) * PL];
-        PLN(a.b.e_vel, 1)[p] += f[(b + 1) * PL];
-        for (int q = 0; q < 4; ++q) PLN(a.b.e_ste, q)[p] += f[(b + 2 + q) * PL];
-        a.b.e_dam[p] += f[(b + 6) * PL];
-        for (int q = 0; q < 10; ++q) f[(b + q) * PL] = 0.0;
-        any = true;
     }
     if (!any) return;
-    // forward flux of this cell
-    double vof[2] = {c.f.m_vof[p], PLN(c.f.m_vof, 1)[p]};
+    // forward flux of this cell; the arrays are kept per role (primary P, other O) so that no
+    // local array is indexed by the run-time material number
     const double evol = c.f.e_vol[p];
-    int prim = 0;
-    double vprim = vof[0];
-    if (vof[0] < SALEC_TOLVOF && vof[1] > vprim) { prim = 1; vprim = vof[1]; }
+    const bool p1 = prim == 1;
     const int other = 1 - prim;
+    const double vother = p1 ? vof[0] : vof[1];
     const double sg[4] = {1.0, 1.0, -1.0, -1.0};
-    double mv[4];
-    for (int k = 0; k < 4; ++k) mv[k] = dmin(vol[k], 0.0);
-    double flux[2][4], fpv[4] = {1., 1., 1., 1.}, fnp[4] = {0., 0., 0., 0.};
-    const bool full = vprim > 1.0 - SALEC_TOLVOF;
+    double mv[4], gP[4], gO[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        mv[k] = dmin(vol[k], 0.0);
+        gP[k] = p1 ? g1[k] : g0[k];
+        gO[k] = p1 ? g0[k] : g1[k];
+    }
+    double fP[4], fO[4], fpv[4] = {1., 1., 1., 1.}, fnp[4] = {0., 0., 0., 0.};
     Dual<5> fpd[4];
     bool fnp_ratio[4] = {false, false, false, false};
-    if (full) {
-        for (int k = 0; k < 4; ++k) { flux[prim][k] = sg[k] * mv[k]; flux[other][k] = 0.0; }
+    if (!CUT) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { fP[k] = sg[k] * mv[k]; fO[k] = 0.0; }
     } else {
         // cut line of the primary material on dual numbers over its four vertex fractions and its
         // cell fraction
@@ -696,7 +752,7 @@ __global__ void ka_flux(const AdjCtx a)
         // fractions of the other material: with one material beside vacuum, the MSTACS
         // fraction divided by its own sum is 1 where that sum exceeds TOLVOF, else the content
         // ratio
-        if (other >= 1) {
+        if (!p1) {
             double cr = dmin(vol[0], 0.0) + dmin(vol[2], 0) + dmin(vol[1], 0) + dmin(vol[3], 0);
             cr = fabs(cr) / evol;
             const double *vvo = PLN(c.f.v_vof, other);
@@ -719,59 +775,81 @@ __global__ void ka_flux(const AdjCtx a)
             const double up[4] = {ev[nb[0]], ev[nb[1]], ev[nb[2]], ev[nb[3]]};
             const double ac[4] = {up[2], up[3], up[0], up[1]};
             for (int k = 0; k < 4; ++k) {
-                const double ar = algebraic_ratio(up[k], vof[other], ac[k], cr, fnx[k], fny[k], ngx, ngy);
+                const double ar = algebraic_ratio(up[k], vother, ac[k], cr, fnx[k], fny[k], ngx, ngy);
                 if (ar > SALEC_TOLVOF) fnp[k] = ar / ar;
-                else { fnp[k] = vof[other] / (1.0 - vprim); fnp_ratio[k] = true; }
+                else { fnp[k] = vother / (1.0 - vprim); fnp_ratio[k] = true; }
             }
         }
+#pragma unroll
         for (int k = 0; k < 4; ++k) {
-            flux[prim][k] = sg[k] * mv[k] * fpv[k];
-            flux[other][k] = sg[k] * mv[k] * (1.0 - fpv[k]) * fnp[k];
+            fP[k] = sg[k] * mv[k] * fpv[k];
+            fO[k] = sg[k] * mv[k] * (1.0 - fpv[k]) * fnp[k];
         }
     }
     // the content cap of material 1
-    double gvof[2] = {0., 0.};
+    double gvP = 0., gvO = 0.;
     {
-        const int m = 1;
+        double F1[4], G1[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { F1[k] = p1 ? fP[k] : fO[k]; G1[k] = p1 ? gP[k] : gO[k]; }
         double d = 0.;
-        d += flux[m][0] * 1.0; d += flux[m][1] * 1.0; d += flux[m][2] * -1.0; d += flux[m][3] * -1.0;
+        d += F1[0] * 1.0; d += F1[1] * 1.0; d += F1[2] * -1.0; d += F1[3] * -1.0;
         const double out = -1.0 * d;
-        if (out > vof[m] * evol) {
-            const double s = vof[m] * evol / out;
+        if (out > vof[1] * evol) {
+            const double s = vof[1] * evol / out;
             double G = 0.;
-            for (int k = 0; k < 4; ++k) G += gflux[m][k] * flux[m][k];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) G += G1[k] * F1[k];
             const double gout = -G * s / out;
             const double dout[4] = {-1.0, -1.0, 1.0, 1.0};
-            for (int k = 0; k < 4; ++k) gflux[m][k] = gflux[m][k] * s + gout * dout[k];
-            gvof[m] += G * evol / out;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double gk = G1[k] * s + gout * dout[k];
+                if (p1) gP[k] = gk;
+                else gO[k] = gk;
+            }
+            if (p1) gvP += G * evol / out;
+            else gvO += G * evol / out;
         }
     }
     // back through the flux formulas to the swept volumes and the cut line
     double gvol[4] = {0., 0., 0., 0.};
-    if (full) {
+    if (!CUT) {
+#pragma unroll
         for (int k = 0; k < 4; ++k)
-            if (vol[k] < 0.) gvol[k] += gflux[prim][k] * sg[k];
+            if (vol[k] < 0.) gvol[k] += gP[k] * sg[k];
     } else {
         double gfp[4];
+#pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const double gmv = sg[k] * (gflux[prim][k] * fpv[k] + gflux[other][k] * (1.0 - fpv[k]) * fnp[k]);
+            const double gmv = sg[k] * (gP[k] * fpv[k] + gO[k] * (1.0 - fpv[k]) * fnp[k]);
             if (vol[k] < 0.) gvol[k] += gmv;
-            gfp[k] = sg[k] * mv[k] * (gflux[prim][k] - gflux[other][k] * fnp[k]);
-            if (other >= 1 && fnp_ratio[k]) {
-                const double gfn = sg[k] * mv[k] * (1.0 - fpv[k]) * gflux[other][k];
-                gvof[other] += gfn / (1.0 - vprim);
-                gvof[prim] += gfn * vof[other] / ((1.0 - vprim) * (1.0 - vprim));
+            gfp[k] = sg[k] * mv[k] * (gP[k] - gO[k] * fnp[k]);
+            if (!p1 && fnp_ratio[k]) {
+                const double gfn = sg[k] * mv[k] * (1.0 - fpv[k]) * gO[k];
+                gvO += gfn / (1.0 - vprim);
+                gvP += gfn * vother / ((1.0 - vprim) * (1.0 - vprim));
             }
         }
         double gvq[5] = {0., 0., 0., 0., 0.};
+#pragma unroll
         for (int k = 0; k < 4; ++k)
+#pragma unroll
             for (int q = 0; q < 5; ++q) gvq[q] += gfp[k] * fpd[k].d[q];
-        for (int k = 0; k < 4; ++k) add(PLN(a.b.v_vof, prim) + vl[k], gvq[k]);
-        gvof[prim] += gvq[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (prim == 0) corner[8 + 2 * k] = gvq[k];
+            else corner[9 + 2 * k] = gvq[k];
+        }
+        gvP += gvq[4];
     }
-    for (int m = 0; m < 2; ++m)
-        if (gvof[m] != 0.0) PLN(a.b.m_vof, m)[p] += gvof[m];
+    {
+        const double gv0 = p1 ? gvO : gvP, gv1 = p1 ? gvP : gvO;
+        if (gv0 != 0.0) a.b.m_vof[p] += gv0;
+        if (gv1 != 0.0) PLN(a.b.m_vof, 1)[p] += gv1;
+    }
     double gd[4][2] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+#pragma unroll
     for (int k = 0; k < 4; ++k) {
         if (gvol[k] == 0.0) continue;
         double o[4];
@@ -781,9 +859,31 @@ __global__ void ka_flux(const AdjCtx a)
         gd[fb[k]][0] += o[2]; gd[fb[k]][1] += o[3];
     }
     for (int k = 0; k < 4; ++k) {
-        add(a.b.v_dis + vl[k], gd[k][0]);
-        add(PLN(a.b.v_dis, 1) + vl[k], gd[k][1]);
+        corner[2 * k] = gd[k][0];
+        corner[2 * k + 1] = gd[k][1];
     }
+}
+
+// the light instance writes every cell's corner scratch (zeros for cut cells), the cut instance
+// then overwrites the cut cells'
+template <bool CUT>
+__global__ void __launch_bounds__(128, CUT ? 1 : 5) ka_flux(const AdjCtx a)
+{
+    const Ctx &c = a.c;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= c.d.enx || j >= c.d.eny) return;
+    const long long p = KIDX(i, j);
+    if (CUT) {
+        const double v0 = c.f.m_vof[p], v1 = PLN(c.f.m_vof, 1)[p];
+        const double vprim = (v0 < SALEC_TOLVOF && v1 > v0) ? v1 : v0;
+        if (vprim > 1.0 - SALEC_TOLVOF) return;
+    }
+    double corner[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) corner[q] = 0.;
+    flux_adj<CUT>(a, i, j, corner);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) a.scr[q * c.d.PL + p] = corner[q];
 }
 
 // ---------------------------------------------------------------- phase 14: remap and EOS
@@ -1096,6 +1196,54 @@ __global__ void ka_gather(AdjGatherArgs A, int stage, double *scratch)
     }
 }
 
+// The forward gather's semantics are parallel: every destination takes op(source) of the values
+// before the gather. Where no reading entry's source is a destination, entries are independent:
+// one thread moves its destination's adjoint to its source (atomically: sources are shared).
+// Where sources include destinations, the map comes as connected components of the
+// destination/source relation, one per thread, disjoint in their points: the thread reads all
+// destination adjoints of its component, clears them, then adds to the sources, without atomics.
+__global__ void ka_gather_fused(AdjGatherArgs A)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= A.g.total) return;
+    int f = 0;
+    while (f + 1 < A.g.nfield && t >= A.g.start[f + 1]) ++f;
+    const GatherField &gf = A.g.field[f];
+    const int k = t - A.g.start[f];
+    const double *fwd = static_cast<const double *>(gf.base);
+    double *adj = A.adj[f];
+    if (gf.cstart) {
+        const int a = gf.cstart[k], b = gf.cstart[k + 1];
+        for (int comp = 0; comp < gf.ncomp; ++comp) {
+            const long long off = (long long)comp * gf.plane;
+            double g[SALEC_GATHER_MAX_COMPONENT];
+#pragma unroll
+            for (int e = 0; e < SALEC_GATHER_MAX_COMPONENT; ++e)
+                if (a + e < b) g[e] = adj[off + gf.dst[a + e]];
+#pragma unroll
+            for (int e = 0; e < SALEC_GATHER_MAX_COMPONENT; ++e)
+                if (a + e < b) adj[off + gf.dst[a + e]] = 0.0;
+#pragma unroll
+            for (int e = 0; e < SALEC_GATHER_MAX_COMPONENT; ++e)
+                if (a + e < b) {
+                    const int src = gf.src[a + e];
+                    const double gv = g[e] * op_deriv((gf.ops[a + e] >> (3 * comp)) & 7u, fwd[off + src]);
+                    if (gv != 0.0) adj[off + src] += gv;
+                }
+        }
+    } else {
+        const int d = gf.dst[k], src = gf.src[k];
+        const unsigned ops = gf.ops[k];
+        for (int comp = 0; comp < gf.ncomp; ++comp) {
+            const long long off = (long long)comp * gf.plane;
+            const double g = adj[off + d];
+            adj[off + d] = 0.0;
+            const double gv = g * op_deriv((ops >> (3 * comp)) & 7u, fwd[off + src]);
+            if (gv != 0.0) atomicAdd(adj + off + src, gv);
+        }
+    }
+}
+
 // ---------------------------------------------------------------- surface-profile misfit
 // per interior column: h = sum over interior rows of (1 - m_vof[0]) * e_pos[3]
 __global__ void ka_profile_height(const Ctx c, double *h)
@@ -1110,8 +1258,7 @@ __global__ void ka_profile_height(const Ctx c, double *h)
     h[i - 2] = s;
 }
 
-__global__ void ka_profile_seed(const Ctx c, const Fields b, const double *h, const double *target, const double *w,
-                                double *J)
+__global__ void ka_profile_seed(const Ctx c, const Fields b, const double *h, const double *target, const double *w)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i < 2 || i > c.d.enx - 3 || j < 2 || j > c.d.eny - 3) return;
@@ -1119,24 +1266,50 @@ __global__ void ka_profile_seed(const Ctx c, const Fields b, const double *h, co
     const double r = h[col] - target[col];
     const long long p = KIDX(i, j);
     b.m_vof[p] += -w[col] * r * PLN(c.f.e_pos, 3)[p];
-    if (j == 2) atomicAdd(J, 0.5 * w[col] * r * r);
 }
 
-__global__ void ka_list_copy(const CopySeg *segs, int nseg, char *base, const long long *slot,
-                             unsigned long long stride, int save)
+// J = 0.5 sum_i w_i r_i^2 in a fixed order (one block: strided partial sums, then a tree), so
+// that the misfit is the same bits on every run
+__global__ void ka_profile_sum(const double *h, const double *target, const double *w, int ncols, double *J)
 {
-    char *rec = base + (slot ? (unsigned long long)*slot * stride : 0ULL);
-    const unsigned long long t0 = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned long long nt = (unsigned long long)gridDim.x * blockDim.x;
-    for (int k = 0; k < nseg; ++k) {
-        const CopySeg g = segs[k];
-        char *dst = save ? rec + g.off : g.field;
-        const char *src = save ? g.field : rec + g.off;
-        const unsigned long long n16 = g.bytes >> 4;
-        for (unsigned long long q = t0; q < n16; q += nt)
-            reinterpret_cast<uint4 *>(dst)[q] = reinterpret_cast<const uint4 *>(src)[q];
-        for (unsigned long long q = (n16 << 4) + t0; q < g.bytes; q += nt) dst[q] = src[q];
+    __shared__ double part[256];
+    double s = 0.;
+    for (int col = threadIdx.x; col < ncols; col += 256) {
+        const double r = h[col] - target[col];
+        s += 0.5 * w[col] * r * r;
     }
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *J = part[0];
+}
+
+__global__ void ka_list_copy(const CopySeg *segs, char *base, const long long *slot, unsigned long long stride,
+                             int save)
+{
+    // blockIdx.y: the field; the x-blocks stride over its 16-byte words, four in flight per thread
+    char *rec = base + (slot ? (unsigned long long)*slot * stride : 0ULL);
+    const CopySeg g = segs[blockIdx.y];
+    char *dst = save ? rec + g.off : g.field;
+    const char *src = save ? g.field : rec + g.off;
+    const unsigned long long n16 = g.bytes >> 4;
+    const unsigned long long nt = (unsigned long long)gridDim.x * blockDim.x;
+    uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+    unsigned long long q = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; q + 3 * nt < n16; q += 4 * nt) {
+        const uint4 a0 = s4[q], a1 = s4[q + nt], a2 = s4[q + 2 * nt], a3 = s4[q + 3 * nt];
+        d4[q] = a0;
+        d4[q + nt] = a1;
+        d4[q + 2 * nt] = a2;
+        d4[q + 3 * nt] = a3;
+    }
+    for (; q < n16; q += nt) d4[q] = s4[q];
+    if (blockIdx.x == 0)
+        for (unsigned long long b = (n16 << 4) + threadIdx.x; b < g.bytes; b += blockDim.x) dst[b] = src[b];
 }
 
 __global__ void ka_slot(long long *slot, long long v, int add)
@@ -1146,10 +1319,16 @@ __global__ void ka_slot(long long *slot, long long v, int add)
 
 } // namespace
 
-void launch_list_copy(const CopySeg *segs, int nseg, char *base, const long long *slot, unsigned long long stride,
-                      bool save, cudaStream_t s)
+void launch_list_copy(const CopySeg *segs, int nseg, unsigned long long max_bytes, char *base, const long long *slot,
+                      unsigned long long stride, bool save, cudaStream_t s)
 {
-    ka_list_copy<<<4 * 148, 256, 0, s>>>(segs, nseg, base, slot, stride, save ? 1 : 0);
+    // about four 16-byte words per thread of the largest field, at most 8 blocks per SM in all
+    const unsigned long long words = (max_bytes + 15) >> 4;
+    unsigned long long bx = (words + 4 * 256 - 1) / (4 * 256);
+    const unsigned long long cap = (unsigned long long)(8 * 148 + nseg - 1) / nseg;
+    if (bx > cap) bx = cap;
+    if (bx < 1) bx = 1;
+    ka_list_copy<<<dim3((unsigned)bx, (unsigned)nseg), 256, 0, s>>>(segs, base, slot, stride, save ? 1 : 0);
 }
 
 void launch_slot_set(long long *slot, long long value, cudaStream_t s) { ka_slot<<<1, 32, 0, s>>>(slot, value, 0); }
@@ -1165,18 +1344,26 @@ void launch_adjoint_kernel(AdjKernel k, const AdjCtx &a, cudaStream_t s)
     case AK_VERTEX_MOMENTUM: ka_vertex_momentum<<<gv, blk, 0, s>>>(a); break;
     case AK_CELL_VELOCITY: ka_cell_velocity<<<g, blk, 0, s>>>(a); break;
     case AK_VOID_VERTICES: ka_void_vertices<<<gv, blk, 0, s>>>(a); break;
-    case AK_GRADIENT: ka_gradient<<<g, blk, 0, s>>>(a); break;
+    case AK_GRADIENT:
+        ka_gradient<<<g, blk, 0, s>>>(a);
+        ka_corner_sum<<<gv, blk, 0, s>>>(a, a.b.v_vel, 0);
+        break;
     case AK_STRESS: ka_stress<<<g, blk, 0, s>>>(a); break;
     case AK_ACCELERATION: ka_acceleration<<<gv, blk, 0, s>>>(a); break;
     case AK_DISPLACEMENT: ka_displacement<<<gv, blk, 0, s>>>(a); break;
     case AK_ENERGY: ka_energy<<<g, blk, 0, s>>>(a); break;
-    case AK_FLUX: ka_flux<<<g, blk, 0, s>>>(a); break;
+    case AK_FLUX:
+        ka_flux<false><<<g, blk, 0, s>>>(a);
+        ka_flux<true><<<g, blk, 0, s>>>(a);
+        ka_corner_sum<<<gv, blk, 0, s>>>(a, a.b.v_dis, 0);
+        ka_corner_sum<<<gv, blk, 0, s>>>(a, a.b.v_vof, 8);
+        break;
     case AK_REMAP_STATE: ka_remap_state<<<g, blk, 0, s>>>(a); break;
     }
 }
 
 void launch_adjoint_gather(const GatherBatch &g, const int *entries, const void *const *adj_base, double *scratch,
-                           cudaStream_t s)
+                           bool two_pass, cudaStream_t s)
 {
     AdjGatherArgs A;
     A.g = g;
@@ -1187,7 +1374,12 @@ void launch_adjoint_gather(const GatherBatch &g, const int *entries, const void 
     }
     const int n = A.estart[g.nfield];
     if (n == 0) return;
-    const int tb = 256, nb = (n + tb - 1) / tb;
+    const int tb = 256;
+    if (!two_pass) {
+        ka_gather_fused<<<(g.total + tb - 1) / tb, tb, 0, s>>>(A);
+        return;
+    }
+    const int nb = (n + tb - 1) / tb;
     for (int stage = 0; stage < 3; ++stage) ka_gather<<<nb, tb, 0, s>>>(A, stage, scratch);
 }
 
@@ -1197,7 +1389,8 @@ void launch_profile_misfit(const Ctx &c, const Fields &b, const double *target, 
     ka_profile_height<<<(c.d.enx + 127) / 128, 128, 0, s>>>(c, h);
     const dim3 blk(32, 4);
     const dim3 g((c.d.enx + blk.x - 1) / blk.x, (c.d.eny + blk.y - 1) / blk.y);
-    ka_profile_seed<<<g, blk, 0, s>>>(c, b, h, target, weight, J);
+    ka_profile_seed<<<g, blk, 0, s>>>(c, b, h, target, weight);
+    ka_profile_sum<<<1, 256, 0, s>>>(h, target, weight, c.d.enx - 4, J);
 }
 
 } // namespace salec

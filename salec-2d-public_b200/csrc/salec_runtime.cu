@@ -1411,6 +1411,7 @@ struct AdjointState {
     Fields b{};
     double *theta = nullptr;       // d/d Yint0, Yfricint, Ydam0, Yfricdam of material 1
     double *gscratch = nullptr;    // reverse-gather scratch
+    double *cscr = nullptr;        // per-cell corner scratch of the reverse sweeps (16 planes)
     size_t gscratch_doubles = 0;
     char *tmp = nullptr;           // forward fields of a phase kept while it is reversed
     size_t tmp_bytes = 0;
@@ -1423,6 +1424,7 @@ struct AdjointState {
     struct ListCopy {
         CopySeg *dev = nullptr;
         int n = 0;
+        unsigned long long max_bytes = 0;
     };
     std::map<std::string, ListCopy> lists;   // device tables of the field lists copied to logs
     long long *slot = nullptr;     // undo-log record of the cycle being replayed or reversed
@@ -1440,31 +1442,31 @@ const char *const kAdjSnapshot[] = {"e_ejt", "m_vof", "e_dvel", "e_den", "v_vof"
                                     "e_strength", "e_vib", "e_pre", "v_acc", "v_alpha", "v_dis", "m_eng", "e_cvs",
                                     "m_pty", "e_wpt", "m_den", "e_cnd", "e_csd", "e_tem", "e_mu", "e_alpha", "e_beta",
                                     "y_profile"};
-// fields each phase writes (its undo log), face records excepted: every face is rewritten by its
-// donor cell in phase 12 before phase 14 reads it
+// fields each phase writes that a reverse sweep or a recipe of the reverse reads (its undo log),
+// face records excepted: every face is rewritten by its donor cell in phase 12 before phase 14
+// reads it. Fields the adjoint's configuration leaves unused (porosity, damping auxiliaries,
+// vibration, ejecta times, lubrication counts, the surface profile) or that only the forward
+// reads (the strength, the plastic strain and its invariant, the vertex damping factor) are not
+// logged: the checkpoints carry them for the replays
 const std::vector<const char *> kAdjWrites[16] = {
-    {"y_profile", "e_ejt"},
+    {},
     {"m_vof", "e_dvel", "e_den", "v_vof", "v_vel", "v_mass"},
     {},
     {"e_vel"},
     {"v_vel"},
     {"e_grad_vel", "e_div_vel", "e_q"},
     {},
-    {"e_ste", "e_ste2s", "e_sta2s", "e_tps", "e_dam", "e_strength", "e_vib"},
-    {"e_pre", "e_ste", "e_q", "v_acc", "v_alpha"},
+    {"e_ste", "e_ste2s", "e_dam"},
+    {"e_pre", "e_ste", "e_q", "v_acc"},
     {"v_dis", "v_vel"},
-    {"m_eng", "e_cvs", "m_pty"},
+    {"m_eng"},
     {},
-    {"e_wpt", "m_den", "e_vib", "m_eng", "m_pty", "e_cvs"},
-    {"e_cnd"},
-    {"m_vof", "m_den", "m_eng", "m_pty", "e_dvel", "e_ste", "e_dam", "e_tps", "e_vib", "e_ejt", "e_den", "e_pre",
-     "e_csd", "e_tem", "e_mu", "e_alpha", "e_beta", "e_cvs"},
+    {"e_wpt", "m_den", "m_eng"},
+    {},
+    {"m_vof", "m_den", "m_eng", "e_dvel", "e_ste", "e_dam", "e_den", "e_pre", "e_csd", "e_tem", "e_mu"},
     {},
 };
 
-// face flux records written by phase 12 and read by phase 14 and its reverse (the face normals
-// are fixed at start-up)
-const std::vector<const char *> kAdjFaces = {"bx_phi", "by_phi"};
 
 size_t field_bytes(const salec_gpu *h, int k)
 {
@@ -1514,6 +1516,24 @@ const AdjointState::ListCopy *list_table(salec_gpu *h, const std::vector<const c
         return nullptr;
     }
     L.n = (int)segs.size();
+    for (const CopySeg &g : segs) L.max_bytes = std::max(L.max_bytes, g.bytes);
+    return &(st->lists[key] = L);
+}
+
+// device table of explicit segments under a key (built outside stream capture)
+const AdjointState::ListCopy *seg_table(salec_gpu *h, const std::string &key, const std::vector<CopySeg> &segs)
+{
+    AdjointState *st = h->adj;
+    auto it = st->lists.find(key);
+    if (it != st->lists.end()) return &it->second;
+    AdjointState::ListCopy L;
+    if (cudaMalloc(reinterpret_cast<void **>(&L.dev), segs.size() * sizeof(CopySeg)) != cudaSuccess) return nullptr;
+    if (cudaMemcpy(L.dev, segs.data(), segs.size() * sizeof(CopySeg), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(L.dev);
+        return nullptr;
+    }
+    L.n = (int)segs.size();
+    for (const CopySeg &g : segs) L.max_bytes = std::max(L.max_bytes, g.bytes);
     return &(st->lists[key] = L);
 }
 
@@ -1524,7 +1544,7 @@ int copy_list(salec_gpu *h, const std::vector<const char *> &names, char *buf, b
 {
     const AdjointState::ListCopy *L = list_table(h, names);
     if (!L) return fail(SALEC_ERR_CUDA, "adjoint: list table unavailable");
-    launch_list_copy(L->dev, L->n, buf, slot, stride, save, h->stream);
+    launch_list_copy(L->dev, L->n, L->max_bytes, buf, slot, stride, save, h->stream);
     CUDA_TRY(cudaGetLastError());
     return SALEC_OK;
 }
@@ -1549,6 +1569,7 @@ void adjoint_release(salec_gpu *h)
     cudaFree(st->pool);
     cudaFree(st->theta);
     cudaFree(st->gscratch);
+    cudaFree(st->cscr);
     cudaFree(st->tmp);
     cudaFree(st->ckpt);
     cudaFree(st->undo);
@@ -1596,13 +1617,14 @@ int adjoint_ensure(salec_gpu *h)
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->gscratch), st->gscratch_doubles * sizeof(double)));
         size_t tb = 0;
         for (int p = 0; p < 16; ++p) tb = std::max(tb, list_bytes(h, kAdjWrites[p]));
+        for (const auto *l : {&kKeep12, &kKeep9, &kKeep8, &kKeep3, &kKeep1}) tb = std::max(tb, list_bytes(h, *l));
         st->tmp_bytes = tb;
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->tmp), tb));
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->slot), sizeof(long long)));
+        CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->cscr), 16 * (size_t)h->d.PL * sizeof(double)));
         // every list table, so that the graphs can be captured
         const std::vector<const char *> snap(std::begin(kAdjSnapshot), std::end(kAdjSnapshot));
-        std::vector<const std::vector<const char *> *> all = {&snap, &kAdjFaces, &kKeep12, &kKeep9, &kKeep8, &kKeep3,
-                                                              &kKeep1};
+        std::vector<const std::vector<const char *> *> all = {&snap, &kKeep12, &kKeep9, &kKeep8, &kKeep3, &kKeep1};
         for (int p = 0; p < 16; ++p) all.push_back(&kAdjWrites[p]);
         for (const auto *l : all)
             if (!list_table(h, *l)) return fail(SALEC_ERR_CUDA, "adjoint: list table");
@@ -1623,7 +1645,7 @@ int adjoint_gather(salec_gpu *h, const Gather &g)
     const void *adj[SALEC_MAX_GATHER_FIELDS];
     for (int f = 0; f < g.batch.nfield; ++f)
         adj[f] = h->adj->pool + (static_cast<char *>(g.batch.field[f].base) - h->pool);
-    launch_adjoint_gather(g.batch, g.entries, adj, h->adj->gscratch, h->stream);
+    launch_adjoint_gather(g.batch, g.entries, adj, h->adj->gscratch, g.two_pass, h->stream);
     CUDA_TRY(cudaGetLastError());
     return SALEC_OK;
 }
@@ -1636,6 +1658,7 @@ int adjoint_phase(salec_gpu *h, int p)
     a.c = h->ctx();
     a.b = st->b;
     a.theta = st->theta;
+    a.scr = st->cscr;
     cudaStream_t s = h->stream;
     const Ctx &c = a.c;
     auto keep = [&](const std::vector<const char *> &names, bool save) { return copy_list(h, names, st->tmp, save); };
@@ -1754,19 +1777,49 @@ int capture_graph(salec_gpu *h, const std::function<int()> &body, cudaGraphExec_
 }
 
 // The two graphs of the window: one cycle replayed with its undo log written to record *slot,
-// and one cycle reversed from record *slot; each moves *slot on by one.
-int adjoint_graphs(salec_gpu *h, size_t ub, const std::vector<size_t> &uoff, size_t fo)
+// and one cycle reversed from record *slot; each moves *slot on by one. The face flux records
+// that the reverse of phase 14 reads are not logged: phase 12 is run again on the state before
+// phase 14, which holds phase 12's inputs unchanged (phase 13 writes only lubrication counts,
+// which the adjoint's configuration leaves off), and rewrites the same records.
+int adjoint_graphs(salec_gpu *h, size_t ub, const std::vector<size_t> &uoff)
 {
     AdjointState *st = h->adj;
     if (st->replay && st->reverse && st->graph_undo == st->undo && st->graph_ub == ub) return SALEC_OK;
     adjoint_drop_graphs(h);
     cudaStream_t s = h->stream;
+    // The undo log of phase p holds its fields and the scalars as they were before phase p. A
+    // field keeps that value from its previous writer in the cycle (or the cycle's start) up to
+    // phase p, so it is saved right after that writer; the scalars change in phases 5 (CFL
+    // candidates), 6 (dt) and 15. The saves of a cycle so fall into a few groups, one copy each.
+    std::vector<std::vector<CopySeg>> groups(17);   // groups[q + 1]: saved after phase q
+    for (int p = 0; p < 16; ++p) {
+        if (kAdjWrites[p].empty()) continue;
+        unsigned long long off = uoff[p];
+        for (const char *n : kAdjWrites[p]) {
+            int q = -1;
+            for (int r = p - 1; r >= 0 && q < 0; --r)
+                for (const char *m : kAdjWrites[r])
+                    if (!strcmp(m, n)) { q = r; break; }
+            const int k = field_by_name(n);
+            const size_t nb = field_bytes(h, k);
+            groups[q + 1].push_back({reinterpret_cast<char *>(field_ptr(h, k)), off, nb});
+            off += nb;
+        }
+        const int qs = p > 6 ? 6 : (p > 5 ? 5 : -1);
+        groups[qs + 1].push_back({reinterpret_cast<char *>(h->scal), off, sizeof(Scal)});
+    }
+    std::vector<const AdjointState::ListCopy *> gtab(17, nullptr);
+    for (int g = 0; g < 17; ++g)
+        if (!groups[g].empty() &&
+            !(gtab[g] = seg_table(h, "save group " + std::to_string(g) + " of " + std::to_string(ub), groups[g])))
+            return fail(SALEC_ERR_CUDA, "adjoint: save table");
     int rc = capture_graph(h, [&]() -> int {
         for (int p = 0; p <= 15; ++p) {
-            if (int r = copy_list(h, kAdjWrites[p], st->undo + uoff[p], true, st->slot, ub)) return r;
+            if (const AdjointState::ListCopy *L = gtab[p]) {
+                launch_list_copy(L->dev, L->n, L->max_bytes, st->undo, st->slot, ub, true, s);
+                CUDA_TRY(cudaGetLastError());
+            }
             if (int r = run_phase(h, p)) return r;
-            if (p == 12)
-                if (int r = copy_list(h, kAdjFaces, st->undo + fo, true, st->slot, ub)) return r;
         }
         launch_slot_add(st->slot, 1, s);
         return SALEC_OK;
@@ -1774,11 +1827,12 @@ int adjoint_graphs(salec_gpu *h, size_t ub, const std::vector<size_t> &uoff, siz
     if (rc) return rc;
     rc = capture_graph(h, [&]() -> int {
         for (int p = 15; p >= 0; --p) {
-            // the faces first: their record carries the scalars after phase 12, which the undo
-            // log of phase 14 then sets back to those before phase 14
+            // a phase without a log changes neither a logged field nor (phases 0, 2, 11, 13) the
+            // scalars; the scalars phases 6 and 15 change are set back by the next log restored
+            if (!kAdjWrites[p].empty())
+                if (int r = copy_list(h, kAdjWrites[p], st->undo + uoff[p], false, st->slot, ub)) return r;
             if (p == 14)
-                if (int r = copy_list(h, kAdjFaces, st->undo + fo, false, st->slot, ub)) return r;
-            if (int r = copy_list(h, kAdjWrites[p], st->undo + uoff[p], false, st->slot, ub)) return r;
+                if (int r = run_phase(h, 12)) return r;
             if (int r = adjoint_phase(h, p)) return r;
         }
         launch_slot_add(st->slot, -1, s);
@@ -1880,10 +1934,6 @@ int salec_gpu_adjoint_window(salec_gpu *h, int nsteps, int every, const double *
     size_t ub = 0;
     std::vector<size_t> uoff(16);
     for (int p = 0; p < 16; ++p) { uoff[p] = ub; ub += list_bytes(h, kAdjWrites[p]); }
-    // the face flux records phase 12 leaves for phase 14 are kept per replayed cycle: the
-    // reverse of cycle k reads cycle k's, not the last replayed cycle's
-    const size_t fo = ub;
-    ub += list_bytes(h, kAdjFaces);
     // buffers: nseg + 1 checkpoints (the last is the window's end), `every` undo logs
     const size_t need_ck = sb * (nseg + 1), need_ud = ub * every;
     if (st->ckpt_bytes < need_ck) {
@@ -1907,7 +1957,7 @@ int salec_gpu_adjoint_window(salec_gpu *h, int nsteps, int every, const double *
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->mis), md * sizeof(double)));
         st->mis_doubles = md;
     }
-    if (int rc = adjoint_graphs(h, ub, uoff, fo)) return rc;
+    if (int rc = adjoint_graphs(h, ub, uoff)) return rc;
     // forward window, with a checkpoint at every segment start; the last segment writes its undo
     // logs on the way, so that it is reversed without a replay
     for (int sgm = 0; sgm < nseg; ++sgm) {
