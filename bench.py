@@ -898,7 +898,20 @@ def run_adjoint(args):
     ev[3].record(stream)
     ev[3].synchronize()
     adj_ms = ev[2].elapsed_time(ev[3])
-    adj_ms_max, fwd_ms_max = ranks.all_max(adj_ms), ranks.all_max(fwd_ms)
+    # the same window as one segment: every cycle's undo log is written during the forward pass
+    # and nothing is replayed (the logs of the whole window fit in HBM at this size)
+    restore(sim, init_state)
+    sim.adjoint_window(args.adj_steps, args.adj_steps, target, density=False)
+    restore(sim, init_state)
+    sim.sync()
+    ranks.barrier()
+    ev[2].record(stream)
+    J1, dp1, dvs1, _ = sim.adjoint_window(args.adj_steps, args.adj_steps, target, density=False)
+    ev[3].record(stream)
+    ev[3].synchronize()
+    adj1_ms = ev[2].elapsed_time(ev[3])
+    same = bool(J1 == J and abs(dvs1 - dvs) <= 1e-9 * abs(dvs))
+    adj_ms_max, fwd_ms_max, adj1_ms_max = ranks.all_max(adj_ms), ranks.all_max(fwd_ms), ranks.all_max(adj1_ms)
     sim.close()
 
     def fd_run(kw, edit=None):
@@ -959,6 +972,8 @@ def run_adjoint(args):
                        "timing": "CUDA events on the library's stream: forward window of --adj-steps cycles vs "
                                  "salec_gpu_adjoint_window (its forward pass, checkpoints, replays and reverse sweeps)"},
             "forward_ms": fwd_ms_max, "adjoint_ms": adj_ms_max,
+            "single_segment": {"adjoint_ms": adj1_ms_max, "ratio": adj1_ms_max / fwd_ms_max,
+                               "same_gradients": same},
             "forward_cell_updates_per_s": world * cells * args.adj_steps / (fwd_ms_max / 1000.0),
             "misfit": J, "misfit_forward": J_fwd,
             "gradients": {"adjoint": adj, "finite_difference": fd, "rel_err": rel,
