@@ -328,7 +328,7 @@ int run_phase_t(salec_gpu *h, int ph)
     const CtxT<R> c = h->ctx_t<R>();
     cudaStream_t s = h->stream;
     int rc = SALEC_OK;
-    static const int kLaunches[16] = {3, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1, 0, 2, 0, 1, 1};
+    static const int kLaunches[16] = {3, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1, 0, 1, 1};
     h->launches += kLaunches[ph] + (ph == 11 && h->tr.n > 0 ? 1 : 0);
     switch (ph) {
     case 0:
@@ -371,10 +371,9 @@ int run_phase_t(salec_gpu *h, int ph)
             launch_step_kernel(SK_TRACERS, c, s, h->blk[SK_TRACERS]);
         }
         break;
-    case 12:
-        launch_step_kernel(SK_FLUX, c, s, h->blk[SK_FLUX], 0);
+    case 12:   // ghost fills of the donor state, then the fluxes of every cell in one launch
         rc = run_gather(h, h->g_flux_state);
-        launch_step_kernel(SK_FLUX, c, s, h->blk[SK_FLUX], (h->d.enx >= 5 && h->d.eny >= 5) ? 2 : 1);
+        launch_step_kernel(SK_FLUX, c, s, h->blk[SK_FLUX], 3);
         break;
     case 13:   // strength condition: count the lubricating tracers of every cell in e_cnd
         if (h->fork_tracers && h->tr.n > 0) CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));

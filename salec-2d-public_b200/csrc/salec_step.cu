@@ -1013,7 +1013,11 @@ __device__ __forceinline__ void pad_ring_cell(int t, int enx, int eny, int &i, i
 }
 
 // pass 0: interior cells; pass 1: pad cells (after the ghost fills of m_den, m_eng, ...), over
-// the whole grid; pass 2: the same pad cells, one thread each (1-D grid over the pad ring).
+// the whole grid; pass 2: the same pad cells, one thread each (1-D grid over the pad ring);
+// pass 3: every cell, after the ghost fills. No cell's flux reads a ghost member the fills write
+// except the pad cells' own, and no flux writes what the fills read, so pass 3 computes what
+// passes 0 and 2 around the fills compute, in one launch whose pad cells hide in the interior's
+// waves.
 template <class R, int NM, bool POR>
 __global__ void SALEC_BOUNDS_FLUX k_flux(const CtxT<R> c, int pass)
 {
@@ -1026,7 +1030,7 @@ __global__ void SALEC_BOUNDS_FLUX k_flux(const CtxT<R> c, int pass)
         i = blockIdx.x * blockDim.x + threadIdx.x;
         j = blockIdx.y * blockDim.y + threadIdx.y;
         if (i >= c.d.enx || j >= c.d.eny) return;
-        if ((pass == 0) != cell_interior(c, i, j)) return;
+        if (pass != 3 && (pass == 0) != cell_interior(c, i, j)) return;
     }
     constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
     const int nmat = NM > 0 ? NM : c.d.nmat;
