@@ -617,7 +617,9 @@ def run_gpu_arm(args):
         mixed = {"value": mvalue, "unit": "cell-updates/s", "ms_per_step": mms / args.steps,
                  "speedup_vs_fp64": mvalue / value,
                  "storage": "FP32 relaxed fields, FP64 m_vof/m_den/m_eng/m_pty/e_cvs/positions/volumes/face records",
-                 "arithmetic": "f64",
+                 "arithmetic": "f32 in the stress update, strength, damage, artificial viscosity, stress "
+                               "divergence and EOS table interpolation; f64 in the Tillotson EOS (mu = rho/rho0 - 1 "
+                               "cancels), remap, fluxes, volume fractions and energies",
                  "rel_l2_vs_fp64": errs, "cycles_compared": total,
                  "fp64_sensitivity_rel_l2": sens,
                  "crater": {"fp64": c64, "mixed": c32,
