@@ -449,8 +449,11 @@ def crater_metrics(e_den: np.ndarray, e_pos: np.ndarray, rho: float, surface: fl
 def run_profile(sim, cycles: int, chunk: int, stream, torch, rho: float, surface: float, dx: float, e_pos):
     """Step `cycles` cycles in chunks; the device time of every chunk from CUDA events recorded
     around it on the library's stream (the sampling between chunks is outside them), and the
-    crater depth and radius after every chunk. Returns the chunk times and the crater history."""
+    crater depth and radius and the compensated conservation sums (salec_gpu_conservation) after
+    every chunk. Returns the chunk times and the history, which starts with the sums before the
+    first chunk."""
     per_chunk, hist = [], []
+    hist.append({"cycle": int(sim.scalar("i_step")), "time_s": sim.scalar("time"), "conservation": sim.conservation()})
     for k in range(cycles // chunk):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
@@ -460,15 +463,31 @@ def run_profile(sim, cycles: int, chunk: int, stream, torch, rho: float, surface
         b.synchronize()
         per_chunk.append(a.elapsed_time(b))
         cm = crater_metrics(sim.get_field("e_den"), e_pos, rho, surface, dx)
-        cm.update({"cycle": int(sim.scalar("i_step")), "time_s": sim.scalar("time")})
+        cm.update({"cycle": int(sim.scalar("i_step")), "time_s": sim.scalar("time"), "conservation": sim.conservation()})
         hist.append(cm)
     return per_chunk, hist
 
 
 def transient(hist):
     """The sample of largest depth: the transient crater (its cycle, time, depth and radius)."""
+    hist = [h for h in hist if "depth_m" in h]
     k = max(range(len(hist)), key=lambda q: hist[q]["depth_m"])
-    return hist[k]
+    return {kk: v for kk, v in hist[k].items() if kk != "conservation"}
+
+
+def conservation_report(hist):
+    """Sums at the run's start and end and their relative change (total energy = internal +
+    kinetic); the per-chunk series stays in the history."""
+    a, b = hist[0]["conservation"], hist[-1]["conservation"]
+
+    def rel(x, y):
+        return (y - x) / abs(x) if x else None
+
+    ea, eb = a["internal_energy"] + a["kinetic_energy"], b["internal_energy"] + b["kinetic_energy"]
+    return {"start": a, "end": b, "summation": "Neumaier-compensated FP64 over the interior cells",
+            "every": "chunk of cycles (see history)",
+            "rel_change": {"mass": rel(a["mass"], b["mass"]), "total_energy": rel(ea, eb),
+                           "momentum_z": rel(a["momentum_z"], b["momentum_z"])}}
 
 
 def run_gpu_arm(args):
@@ -580,7 +599,8 @@ def run_gpu_arm(args):
                  "value": world * cells * args.long_cycles / (all_max(total_ms) / 1000.0),
                  "ms_per_cycle_by_chunk": [round(c / args.chunk, 4) for c in chunks],
                  "late_window": late, "developed_state": dev,
-                 "crater_fp64": {"transient": transient(hist64), "final": hist64[-1]},
+                 "crater_fp64": {"transient": transient(hist64), "final": transient(hist64[-1:])},
+                 "conservation_fp64": conservation_report(hist64),
                  "nonfinite": sim.check()}
 
     # mixed form (FP32 storage of the relaxed fields): same deck, same window, then its state
@@ -655,7 +675,9 @@ def run_gpu_arm(args):
                                      "radius_rel_err": rel(t32["radius_m"], t64["radius_m"]),
                                      "fp64_sensitivity_depth": rel(tp["depth_m"], t64["depth_m"]),
                                      "fp64_sensitivity_radius": rel(tp["radius_m"], t64["radius_m"])},
-                "final_crater": {"fp64": hist64[-1], "mixed": hist32[-1], "fp64_perturbed": histp[-1]},
+                "final_crater": {"fp64": transient(hist64[-1:]), "mixed": transient(hist32[-1:]),
+                                 "fp64_perturbed": transient(histp[-1:])},
+                "conservation": {"fp64": conservation_report(hist64), "mixed": conservation_report(hist32)},
                 "crater_history_fp64": hist64, "crater_history_mixed": hist32,
                 "nonfinite": mix.check() + sim.check()}
         mix.close()
