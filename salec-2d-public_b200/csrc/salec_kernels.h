@@ -59,7 +59,7 @@ enum StepKernel {
     SK_PROFILE_RESET, SK_TRACE_PROFILE, SK_PROFILE_DECODE, SK_VERTEX_VOF_MOMENTUM, SK_CELL_VELOCITY,
     SK_VOID_VERTICES, SK_GRADIENT, SK_FINALIZE_DT, SK_STRESS, SK_ACCELERATION, SK_DISPLACEMENT, SK_ENERGY,
     SK_TRACERS, SK_FLUX, SK_REMAP_DAMP_STATE, SK_CYCLE, SK_RECORD_REFERENCE, SK_INIT_VERTEX_VELOCITY,
-    SK_STRENGTH_CONDITION, SK_LAPLACE_MASK, SK_COUNT
+    SK_STRENGTH_CONDITION, SK_LAPLACE_MASK, SK_STRESS_ENERGY, SK_COUNT
 };
 
 #ifdef __CUDACC__

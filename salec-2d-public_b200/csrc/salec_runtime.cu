@@ -322,14 +322,17 @@ int run_gather(salec_gpu *h, const Gather &g)
     return SALEC_OK;
 }
 
+// fused: the cycle graph's form, in which the stress sweep of phase 7 also does the energy
+// update and phase 10 launches nothing; phase-by-phase callers and the adjoint use the
+// separate sweeps, which compute the same bits
 template <class R>
-int run_phase_t(salec_gpu *h, int ph)
+int run_phase_t(salec_gpu *h, int ph, bool fused)
 {
     const CtxT<R> c = h->ctx_t<R>();
     cudaStream_t s = h->stream;
     int rc = SALEC_OK;
     static const int kLaunches[16] = {3, 1, 0, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1, 0, 1, 1};
-    h->launches += kLaunches[ph] + (ph == 11 && h->tr.n > 0 ? 1 : 0);
+    h->launches += kLaunches[ph] + (ph == 11 && h->tr.n > 0 ? 1 : 0) - (fused && ph == 10 ? 1 : 0);
     switch (ph) {
     case 0:
         launch_step_kernel(SK_PROFILE_RESET, c, s, h->blk[SK_PROFILE_RESET]);
@@ -350,7 +353,7 @@ int run_phase_t(salec_gpu *h, int ph)
     case 4: launch_step_kernel(SK_VOID_VERTICES, c, s, h->blk[SK_VOID_VERTICES]); break;
     case 5: launch_step_kernel(SK_GRADIENT, c, s, h->blk[SK_GRADIENT]); break;
     case 6: launch_step_kernel(SK_FINALIZE_DT, c, s, h->blk[SK_FINALIZE_DT]); break;
-    case 7: launch_step_kernel(SK_STRESS, c, s, h->blk[SK_STRESS]); break;
+    case 7: launch_step_kernel(fused ? SK_STRESS_ENERGY : SK_STRESS, c, s, h->blk[SK_STRESS]); break;
     case 8:
         rc = run_gather(h, h->g_pre_ste_q);
         launch_step_kernel(SK_ACCELERATION, c, s, h->blk[SK_ACCELERATION]);
@@ -360,7 +363,9 @@ int run_phase_t(salec_gpu *h, int ph)
         launch_step_kernel(SK_DISPLACEMENT, c, s, h->blk[SK_DISPLACEMENT]);
         rc = run_gather(h, h->r_dis);
         break;
-    case 10: launch_step_kernel(SK_ENERGY, c, s, h->blk[SK_ENERGY]); break;
+    case 10:
+        if (!fused) launch_step_kernel(SK_ENERGY, c, s, h->blk[SK_ENERGY]);
+        break;
     case 11:
         if (h->fork_tracers && h->tr.n > 0) {
             CUDA_TRY(cudaEventRecord(h->ev_fork, s));
@@ -397,7 +402,10 @@ int run_phase_t(salec_gpu *h, int ph)
     return SALEC_OK;
 }
 
-int run_phase(salec_gpu *h, int ph) { return h->mixed ? run_phase_t<float>(h, ph) : run_phase_t<double>(h, ph); }
+int run_phase(salec_gpu *h, int ph, bool fused = false)
+{
+    return h->mixed ? run_phase_t<float>(h, ph, fused) : run_phase_t<double>(h, ph, fused);
+}
 
 int build_gathers(salec_gpu *h)
 {
@@ -1030,7 +1038,7 @@ void capture_cycle_graph(salec_gpu *h)
     }
     int rc = SALEC_OK;
     h->fork_tracers = true;
-    for (int p = 0; p <= 15 && rc == SALEC_OK; ++p) rc = run_phase(h, p);
+    for (int p = 0; p <= 15 && rc == SALEC_OK; ++p) rc = run_phase(h, p, true);
     h->fork_tracers = false;
     const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     h->launches = before;

@@ -467,6 +467,14 @@ __global__ void __launch_bounds__(SALEC_FINALIZE_THREADS) k_finalize_dt(const Ct
 // ============================================================ phase 7: vibration, stress, damage
 // block_vibration (src/strength.c:625-695) and update_e_stress (src/strength.c:7-349).
 template <class R, int NM, bool POR>
+__device__ __forceinline__ void energy_cell(const CtxT<R> &c, long long p, double s0, double s1, double s2, double s3,
+                                            double g0, double g1, double g2, double g3, double g4, double pre);
+
+// EN: the energy update of phase 10 follows in the same thread (the cycle graph's form). It reads
+// the cell's new stress, its velocity gradient, pressure and viscosity, which phases 8 and 9 do
+// not change for an interior cell, and writes m_eng, m_pty and e_cvs, which they do not read, so
+// it computes what the separate sweep computes after them.
+template <class R, int NM, bool POR, bool EN = false>
 __global__ void SALEC_BOUNDS_STRESS k_stress(const CtxT<R> c)
 {
     using A = R;   // arithmetic of stress, strength and damage: FP64, or FP32 in the mixed form
@@ -668,6 +676,8 @@ __global__ void SALEC_BOUNDS_STRESS k_stress(const CtxT<R> c)
     c.f.e_tps[p] = tps;
     c.f.e_dam[p] = dam;
     c.f.e_strength[p] = strength;
+    if (EN && !(rho < SALEC_TOLRHO))
+        energy_cell<R, NM, POR>(c, p, R(s0), R(s1), R(s2), R(s3), g0, g1, g2, g3, g4, pre);
 }
 
 // ============================================================ phase 8: vertex acceleration
@@ -799,15 +809,14 @@ __global__ void k_vertex_displacement(const CtxT<R> c)
 // ============================================================ phase 10: internal energy
 // update_energy (src/sale2d.c:564-712) with the Wunnemann porosity update. After the vacuum
 // test, every input of the cell is loaded in one batch (no load waits on another).
+// The energy update of one interior cell p that is not vacuum, from the cell's new stress (s),
+// its velocity gradient (g) and pressure as stored (widened from R to FP64).
 template <class R, int NM, bool POR>
-__global__ void SALEC_BOUNDS_ENERGY k_energy(const CtxT<R> c)
+__device__ __forceinline__ void energy_cell(const CtxT<R> &c, long long p, double s0, double s1, double s2, double s3,
+                                            double g0, double g1, double g2, double g3, double g4, double pre)
 {
     constexpr int MM = NM > 0 ? NM : SALEC_MAXMAT;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (!cell_interior(c, i, j)) return;
-    const long long p = KIDX(i, j);
     const int nmat = NM > 0 ? NM : c.d.nmat;
-    if (c.f.m_vof[p] > SALEC_TOLVOF || c.f.e_den[p] < SALEC_TOLRHO) return;
     double vm[MM], rm[MM], em[MM], pt[MM];
     #pragma unroll
     for (int m = 1; m < nmat; ++m) {
@@ -817,12 +826,8 @@ __global__ void SALEC_BOUNDS_ENERGY k_energy(const CtxT<R> c)
         pt[m] = POR ? PLN(c.f.m_pty, m)[p] : 1.0;
     }
     const double dt = c.scal->dt;
-    const double pre = c.f.e_pre[p];
     const double q = c.f.e_q[p];
     const double div = c.f.e_div_vel[p];
-    const double g0 = c.f.e_grad_vel[p], g1 = PLN(c.f.e_grad_vel, 1)[p], g2 = PLN(c.f.e_grad_vel, 2)[p],
-                 g3 = PLN(c.f.e_grad_vel, 3)[p], g4 = PLN(c.f.e_grad_vel, 4)[p];
-    const double s0 = c.f.e_ste[p], s1 = PLN(c.f.e_ste, 1)[p], s2 = PLN(c.f.e_ste, 2)[p], s3 = PLN(c.f.e_ste, 3)[p];
     const double cvs_old = c.f.e_cvs[p];
     double sig = 0., ev0 = 0., ev1 = 0.;
     if (POR) {
@@ -859,6 +864,18 @@ __global__ void SALEC_BOUNDS_ENERGY k_energy(const CtxT<R> c)
     }
     // the reference updates e_cvs for every non-vacuum cell, with or without porosity
     c.f.e_cvs[p] = wind(cvs_old + dcvs * dt, -10.0, 10.0);
+}
+
+template <class R, int NM, bool POR>
+__global__ void SALEC_BOUNDS_ENERGY k_energy(const CtxT<R> c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (!cell_interior(c, i, j)) return;
+    const long long p = KIDX(i, j);
+    if (c.f.m_vof[p] > SALEC_TOLVOF || c.f.e_den[p] < SALEC_TOLRHO) return;
+    energy_cell<R, NM, POR>(c, p, c.f.e_ste[p], PLN(c.f.e_ste, 1)[p], PLN(c.f.e_ste, 2)[p], PLN(c.f.e_ste, 3)[p],
+                            c.f.e_grad_vel[p], PLN(c.f.e_grad_vel, 1)[p], PLN(c.f.e_grad_vel, 2)[p],
+                            PLN(c.f.e_grad_vel, 3)[p], PLN(c.f.e_grad_vel, 4)[p], c.f.e_pre[p]);
 }
 
 // ============================================================ phase 11: tracers
@@ -1970,6 +1987,7 @@ void launch_step_kernel(StepKernel k, const CtxT<R> &c, cudaStream_t s, dim3 b, 
     case SK_GRADIENT: k_gradient_viscosity_cfl<R><<<g, b, 0, s>>>(c); break;
     case SK_FINALIZE_DT: k_finalize_dt<R><<<148, SALEC_FINALIZE_THREADS, 0, s>>>(c); break;
     case SK_STRESS: SALEC_NM_DISPATCH(k_stress, c); break;
+    case SK_STRESS_ENERGY: SALEC_NM_DISPATCH_P3(k_stress, true, c); break;
     case SK_ACCELERATION: k_vertex_acceleration<R><<<gv, b, 0, s>>>(c); break;
     case SK_DISPLACEMENT: k_vertex_displacement<R><<<gv, b, 0, s>>>(c); break;
     case SK_ENERGY: SALEC_NM_DISPATCH(k_energy, c); break;
