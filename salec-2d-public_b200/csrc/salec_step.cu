@@ -55,6 +55,14 @@ namespace salec {
 #ifndef SALEC_REGS_STRESS_F
 #define SALEC_REGS_STRESS_F SALEC_REGS_STRESS
 #endif
+// the stress sweep with the energy update fused (the cycle graph's form): 72 measured best
+// against 56, 64, 80 and 96 (1.2695, 1.2639, 1.2572, 1.2825, 1.2946 ms per cycle at 2048²)
+#ifndef SALEC_REGS_STRESS_EN
+#define SALEC_REGS_STRESS_EN 72
+#endif
+#ifndef SALEC_REGS_STRESS_EN_F
+#define SALEC_REGS_STRESS_EN_F SALEC_REGS_STRESS_EN
+#endif
 #ifndef SALEC_REGS_FLUX_F
 #define SALEC_REGS_FLUX_F SALEC_REGS_FLUX
 #endif
@@ -74,7 +82,9 @@ namespace salec {
 #define SALEC_REGS_GRAD_F SALEC_REGS_GRAD
 #endif
 #if SALEC_REGS_STRESS > 0
-#define SALEC_BOUNDS_STRESS __maxnreg__((sizeof(R) == 4 ? SALEC_REGS_STRESS_F : SALEC_REGS_STRESS))
+#define SALEC_BOUNDS_STRESS                                                                              \
+    __maxnreg__((EN ? (sizeof(R) == 4 ? SALEC_REGS_STRESS_EN_F : SALEC_REGS_STRESS_EN)                  \
+                    : (sizeof(R) == 4 ? SALEC_REGS_STRESS_F : SALEC_REGS_STRESS)))
 #else
 #define SALEC_BOUNDS_STRESS __launch_bounds__(256)
 #endif
