@@ -557,19 +557,24 @@ def run_gpu_arm(args):
     # output field set
     out_fields = fields.OUTPUT_FIELDS
     h2d = sum(a.nbytes for a in snap_start["fields"].values()) + snap_start["tracers"].nbytes
-    d2h_step = 64 + 8 * (n + 4)   # the 64-byte scalar block (dt, time, ...) and the surface profile
+    d2h_step = 80 + 8 * (n + 4)   # the 80-byte scalar block (dt, time, ...) and the surface profile
     d2h_out = sum(8 * np.prod(sim.shape(f)) for f in out_fields)
     out_bufs = {f: torch.empty(int(np.prod(sim.shape(f))), dtype=torch.float64, pin_memory=True).numpy()
                 .reshape(sim.shape(f)) for f in out_fields}
-    prof_buf = torch.empty(int(np.prod(sim.shape("y_profile"))), dtype=torch.float64,
-                           pin_memory=True).numpy().reshape(sim.shape("y_profile"))
+    prof_bufs = [torch.empty(int(np.prod(sim.shape("y_profile"))), dtype=torch.float64,
+                             pin_memory=True).numpy().reshape(sim.shape("y_profile")) for _ in range(2)]
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     restore(sim, snap_start)
     t_up = time.perf_counter()
-    for _ in range(args.steps):
-        sim.step_report(1, prof_buf)   # the cycle, then dt, time and the surface profile
+    # every cycle's dt, time and surface profile are read back; cycle k+1 is queued before the
+    # host waits for cycle k's results (salec_gpu_step_report_async, two report slots)
+    sim.step_report_async(1, prof_bufs[0], 0)
+    for k in range(1, args.steps):
+        sim.step_report_async(1, prof_bufs[k % 2], k % 2)
+        sim.report_wait((k - 1) % 2)
+    sim.report_wait((args.steps - 1) % 2)
     t_loop = time.perf_counter()
     outs = [sim.get_field(f, out=out_bufs[f]) for f in out_fields]
     sim.sync()

@@ -153,6 +153,15 @@ int salec_gpu_step(salec_gpu *h, int nsteps);
  * behind the cycles and the call synchronises once, where salec_gpu_get_scalar and
  * salec_gpu_get_field would synchronise once each. Results equal those calls'. */
 int salec_gpu_step_report(salec_gpu *h, int nsteps, double *dt, double *time, double *profile, long long profile_n);
+/* The same, pipelined: queue nsteps cycles and the read-back of dt, time and (when profile is not
+ * NULL) the surface profile into report slot `slot` (0 or 1), and return without waiting.
+ * salec_gpu_report_wait(h, slot, &dt, &time) then waits for that slot's read-back and gives dt
+ * and time. A host loop can so queue cycle k+1 before it waits for cycle k's results, and the
+ * device does not idle while the host wakes up. profile should be page-locked memory
+ * (cudaHostAlloc) for the copy to overlap; it is written when the slot's wait returns. A slot
+ * must be waited for before it is queued again. */
+int salec_gpu_step_report_async(salec_gpu *h, int nsteps, double *profile, long long profile_n, int slot);
+int salec_gpu_report_wait(salec_gpu *h, int slot, double *dt, double *time);
 /* Advance an ensemble of independent simulations (each handle a different deck or mesh size)
  * by nsteps cycles each. Cycles are queued round-robin, chunk cycles per member at a time, each
  * member on its own stream, so the kernels of small meshes run side by side on the device.

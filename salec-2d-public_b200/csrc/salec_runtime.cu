@@ -165,6 +165,11 @@ struct salec_gpu {
     // reads nothing the flux writes and writes only tracer arrays); joined before phase 13
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // pipelined read-back (salec_gpu_step_report_async): per slot a pinned copy of the scalars,
+    // its completion event and whether it is in flight
+    Scal *report_scal[2] = {nullptr, nullptr};
+    cudaEvent_t report_ev[2] = {nullptr, nullptr};
+    bool report_pending[2] = {false, false};
     bool fork_tracers = false;
     void *output = nullptr;     // output writer state (salec_output.cu)
     void *conserve = nullptr;   // scratch of the conservation sums (salec_conserve.cu)
@@ -732,6 +737,10 @@ void release(salec_gpu *h)
     for (auto e : h->ev_a) cudaEventDestroy(e);
     for (auto e : h->ev_b) cudaEventDestroy(e);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    for (int k = 0; k < 2; ++k) {
+        if (h->report_scal[k]) cudaFreeHost(h->report_scal[k]);
+        if (h->report_ev[k]) cudaEventDestroy(h->report_ev[k]);
+    }
     if (h->ev_join) cudaEventDestroy(h->ev_join);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1110,6 +1119,52 @@ int salec_gpu_step_report(salec_gpu *h, int nsteps, double *dt, double *time, do
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     if (dt) *dt = h->scal_host->dt;
     if (time) *time = h->scal_host->time;
+    return SALEC_OK;
+}
+
+int salec_gpu_step_report_async(salec_gpu *h, int nsteps, double *profile, long long profile_n, int slot)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    if (slot < 0 || slot > 1) return fail(SALEC_ERR_ARG, "report slot must be 0 or 1");
+    if (h->report_pending[slot]) return fail(SALEC_ERR_STATE, "report slot still in flight: wait for it first");
+    const int fid = field_by_name("y_profile");
+    int nx = 0, ny = 0;
+    field_points(h, fid, nx, ny);
+    const long long need = (long long)nx * ny * field_ncomp(h, fid);
+    if (profile && profile_n != need)
+        return fail(SALEC_ERR_ARG, "y_profile: expected " + std::to_string(need) + " doubles, got " +
+                                       std::to_string(profile_n));
+    if (profile) {
+        if (int rc = ensure_staging(h, (size_t)need)) return rc;
+    }
+    if (!h->report_scal[slot]) {
+        CUDA_TRY(cudaMallocHost(reinterpret_cast<void **>(&h->report_scal[slot]), sizeof(Scal)));
+        CUDA_TRY(cudaEventCreateWithFlags(&h->report_ev[slot], cudaEventDisableTiming));
+    }
+    if (int rc = salec_gpu_step(h, nsteps)) return rc;
+    // the copies queue behind the cycles; the staging buffer is reused in stream order
+    CUDA_TRY(cudaMemcpyAsync(h->report_scal[slot], h->scal, sizeof(Scal), cudaMemcpyDeviceToHost, h->stream));
+    if (profile) {
+        const long long plane = kFields[fid].loc == L_COL ? 0 : h->d.PL;
+        launch_planes_to_aos(field_ptr(h, fid), field_f32(h, fid), h->staging, plane, h->d.P, nx, ny,
+                             field_ncomp(h, fid), h->stream);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(profile, h->staging, need * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    CUDA_TRY(cudaEventRecord(h->report_ev[slot], h->stream));
+    h->report_pending[slot] = true;
+    return SALEC_OK;
+}
+
+int salec_gpu_report_wait(salec_gpu *h, int slot, double *dt, double *time)
+{
+    if (!h) return fail(SALEC_ERR_ARG, "null handle");
+    if (slot < 0 || slot > 1) return fail(SALEC_ERR_ARG, "report slot must be 0 or 1");
+    if (!h->report_pending[slot]) return fail(SALEC_ERR_STATE, "report slot not queued");
+    h->report_pending[slot] = false;
+    CUDA_TRY(cudaEventSynchronize(h->report_ev[slot]));
+    if (dt) *dt = h->report_scal[slot]->dt;
+    if (time) *time = h->report_scal[slot]->time;
     return SALEC_OK;
 }
 

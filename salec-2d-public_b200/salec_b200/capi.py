@@ -43,7 +43,7 @@ class AdjointResult(ctypes.Structure):
 
 
 PRECISION_FP64 = 0    # salec_precision: plain FP64 (bit-parity form)
-PRECISION_MIXED = 1   # FP32 storage of the relaxed fields, FP64 arithmetic and conserved fields
+PRECISION_MIXED = 1   # FP32 storage of the relaxed fields, FP32 arithmetic of stress, strength and viscosity
 
 
 MAT_DOUBLES = ["VaporDen", "MeltDen", "GaCoef", "Yint0", "Yfricint", "Ylimint", "Ydam0", "Yfricdam", "Ylimdam",
@@ -93,6 +93,8 @@ def lib() -> ctypes.CDLL:
             "salec_gpu_step": ([vp, c_i], c_i),
             "salec_gpu_step_many": ([ctypes.POINTER(vp), c_i, c_i, c_i], c_i),
             "salec_gpu_step_report": ([vp, c_i, P_D, P_D, P_D, c_ll], c_i),
+            "salec_gpu_step_report_async": ([vp, c_i, P_D, c_ll, c_i], c_i),
+            "salec_gpu_report_wait": ([vp, c_i, P_D, P_D], c_i),
             "salec_gpu_autotune": ([vp, c_i, ctypes.POINTER(c_i)], c_i),
             "salec_gpu_set_block_shapes": ([vp, ctypes.POINTER(c_i), c_i], c_i),
             "salec_gpu_phases": ([vp, c_i, c_i], c_i),
@@ -315,6 +317,23 @@ class Simulation:
             pp, pn = _ptr(profile), profile.size
         _check(lib().salec_gpu_step_report(self.h, int(n), ctypes.byref(dt), ctypes.byref(t), pp, pn),
                "step_report")
+        return dt.value, t.value
+
+    def step_report_async(self, n: int, profile: np.ndarray | None, slot: int) -> None:
+        """Queue step(n) and the read-back of dt, time and the surface profile into report slot
+        `slot` without waiting (salec_gpu_step_report_async); `profile` should be page-locked."""
+        pp, pn = None, 0
+        if profile is not None:
+            shp = self.shape("y_profile")
+            if profile.dtype != np.float64 or tuple(profile.shape) != tuple(shp) or not profile.flags.c_contiguous:
+                raise ValueError("step_report_async: profile must be C-contiguous float64 of shape %s" % (shp,))
+            pp, pn = _ptr(profile), profile.size
+        _check(lib().salec_gpu_step_report_async(self.h, int(n), pp, pn, int(slot)), "step_report_async")
+
+    def report_wait(self, slot: int):
+        """Wait for report slot `slot`; returns (dt, time) of its cycles."""
+        dt, t = c_d(), c_d()
+        _check(lib().salec_gpu_report_wait(self.h, int(slot), ctypes.byref(dt), ctypes.byref(t)), "report_wait")
         return dt.value, t.value
 
     def phases(self, first: int, last: int) -> None:
