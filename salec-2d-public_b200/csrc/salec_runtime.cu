@@ -1881,7 +1881,10 @@ int adjoint_graphs(salec_gpu *h, size_t ub, const std::vector<size_t> &uoff)
                 launch_list_copy(L->dev, L->n, L->max_bytes, st->undo, st->slot, ub, true, s);
                 CUDA_TRY(cudaGetLastError());
             }
-            if (int r = run_phase(h, p)) return r;
+            // the cycle graph's form: the energy update inside phase 7. The logs are the same:
+            // m_eng is saved at the cycle's start for phase 10 and after phase 10 for phase 12,
+            // and phases 8 and 9 leave it alone
+            if (int r = run_phase(h, p, true)) return r;
         }
         launch_slot_add(st->slot, 1, s);
         return SALEC_OK;
