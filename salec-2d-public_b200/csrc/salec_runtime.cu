@@ -1544,12 +1544,11 @@ size_t list_bytes(const salec_gpu *h, const List &names)
     return (b + 255) & ~(size_t)255;
 }
 
-// fields the reverse recipes keep aside while they re-run a forward sub-step
+// fields whose ghost cells the reverse recipes fill again (the gathers inside phases 1, 8 and 12
+// run before the sweep they feed), kept aside and put back afterwards
 const std::vector<const char *> kKeep12 = {"m_den", "e_vib", "m_eng"};
-const std::vector<const char *> kKeep9 = {"v_dis", "v_vel"};
-const std::vector<const char *> kKeep8 = {"e_pre", "e_ste", "e_q", "v_acc"};
-const std::vector<const char *> kKeep3 = {"e_vel"};
-const std::vector<const char *> kKeep1 = {"m_vof", "e_dvel", "e_den", "v_vof", "v_vel", "v_mass"};
+const std::vector<const char *> kKeep8 = {"e_pre", "e_ste", "e_q"};
+const std::vector<const char *> kKeep1 = {"m_vof", "e_dvel", "e_den"};
 
 // Device table of a field list: the fields in order, then the scalar block, at the offsets of
 // list_bytes' record layout. Built outside stream capture (adjoint_tables builds every list).
@@ -1679,14 +1678,14 @@ int adjoint_ensure(salec_gpu *h)
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->gscratch), st->gscratch_doubles * sizeof(double)));
         size_t tb = 0;
         for (int p = 0; p < 16; ++p) tb = std::max(tb, list_bytes(h, kAdjWrites[p]));
-        for (const auto *l : {&kKeep12, &kKeep9, &kKeep8, &kKeep3, &kKeep1}) tb = std::max(tb, list_bytes(h, *l));
+        for (const auto *l : {&kKeep12, &kKeep8, &kKeep1}) tb = std::max(tb, list_bytes(h, *l));
         st->tmp_bytes = tb;
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->tmp), tb));
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->slot), sizeof(long long)));
         CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(&st->cscr), 16 * (size_t)h->d.PL * sizeof(double)));
         // every list table, so that the graphs can be captured
         const std::vector<const char *> snap(std::begin(kAdjSnapshot), std::end(kAdjSnapshot));
-        std::vector<const std::vector<const char *> *> all = {&snap, &kKeep12, &kKeep9, &kKeep8, &kKeep3, &kKeep1};
+        std::vector<const std::vector<const char *> *> all = {&snap, &kKeep12, &kKeep8, &kKeep1};
         for (int p = 0; p < 16; ++p) all.push_back(&kAdjWrites[p]);
         for (const auto *l : all)
             if (!list_table(h, *l)) return fail(SALEC_ERR_CUDA, "adjoint: list table");
@@ -1722,7 +1721,6 @@ int adjoint_phase(salec_gpu *h, int p)
     a.theta = st->theta;
     a.scr = st->cscr;
     cudaStream_t s = h->stream;
-    const Ctx &c = a.c;
     auto keep = [&](const std::vector<const char *> &names, bool save) { return copy_list(h, names, st->tmp, save); };
     int rc = SALEC_OK;
     switch (p) {
@@ -1735,17 +1733,17 @@ int adjoint_phase(salec_gpu *h, int p)
         if ((rc = adjoint_gather(h, h->g_flux_state))) return rc;
         break;
     case 10: launch_adjoint_kernel(AK_ENERGY, a, s); break;
+    // The reverse of a gather needs the forward values only for the ops whose derivative depends
+    // on them (|x|, in the velocity-increment ghosts of phase 1, whose sources are interior and
+    // unchanged by the gather); the restrictions and the other ghost patterns copy, negate or
+    // zero. So no recipe re-runs a sweep to obtain the values a later gather reads.
     case 9:
-        if ((rc = keep(kKeep9, true))) return rc;
-        launch_step_kernel(SK_DISPLACEMENT, c, s, h->blk[SK_DISPLACEMENT]);
         if ((rc = adjoint_gather(h, h->r_dis))) return rc;
-        if ((rc = keep(kKeep9, false))) return rc;
         launch_adjoint_kernel(AK_DISPLACEMENT, a, s);
         break;
     case 8:
         if ((rc = keep(kKeep8, true))) return rc;
         if ((rc = run_gather(h, h->g_pre_ste_q))) return rc;
-        launch_step_kernel(SK_ACCELERATION, c, s, h->blk[SK_ACCELERATION]);
         if ((rc = adjoint_gather(h, h->r_acc))) return rc;
         launch_adjoint_kernel(AK_ACCELERATION, a, s);
         if ((rc = keep(kKeep8, false))) return rc;
@@ -1755,27 +1753,15 @@ int adjoint_phase(salec_gpu *h, int p)
     case 5: launch_adjoint_kernel(AK_GRADIENT, a, s); break;
     case 4: launch_adjoint_kernel(AK_VOID_VERTICES, a, s); break;
     case 3:
-        if ((rc = keep(kKeep3, true))) return rc;
-        launch_step_kernel(SK_CELL_VELOCITY, c, s, h->blk[SK_CELL_VELOCITY]);
         if ((rc = adjoint_gather(h, h->g_evel))) return rc;
-        if ((rc = keep(kKeep3, false))) return rc;
         launch_adjoint_kernel(AK_CELL_VELOCITY, a, s);
         break;
     case 1: {
+        // the sweep reads the cell fields' ghosts as the gathers fill them
         if ((rc = keep(kKeep1, true))) return rc;
         if ((rc = run_gather(h, h->g_mvof))) return rc;
         if ((rc = run_gather(h, h->g_dvel_den))) return rc;
-        launch_step_kernel(SK_VERTEX_VOF_MOMENTUM, c, s, h->blk[SK_VERTEX_VOF_MOMENTUM]);
         if ((rc = adjoint_gather(h, h->r_vel))) return rc;
-        // back to the gathered cell fields with the vertex fields before the sweep
-        size_t off = 0;
-        for (const char *n : {"m_vof", "e_dvel", "e_den"}) off += field_bytes(h, field_by_name(n));
-        for (const char *n : {"v_vof", "v_vel", "v_mass"}) {
-            const int k = field_by_name(n);
-            const size_t nb = field_bytes(h, k);
-            CUDA_TRY(cudaMemcpyAsync(field_ptr(h, k), st->tmp + off, nb, cudaMemcpyDeviceToDevice, s));
-            off += nb;
-        }
         launch_adjoint_kernel(AK_VERTEX_MOMENTUM, a, s);
         if ((rc = keep(kKeep1, false))) return rc;
         if ((rc = adjoint_gather(h, h->g_dvel_den))) return rc;
