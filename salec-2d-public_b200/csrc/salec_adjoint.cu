@@ -1287,19 +1287,20 @@ __global__ void ka_profile_sum(const double *h, const double *target, const doub
     if (threadIdx.x == 0) *J = part[0];
 }
 
-__global__ void ka_list_copy(const CopySeg *segs, char *base, const long long *slot, unsigned long long stride,
-                             int save)
+__global__ void __launch_bounds__(256, 4) ka_list_copy(const CopySeg *segs, char *base, const long long *slot,
+                                                       unsigned long long stride, int save)
 {
-    // blockIdx.y: the field; the x-blocks stride over its 16-byte words, four in flight per thread
+    // blockIdx.y: the field; the x-blocks stride over its 16-byte words (a field is below 2^31
+    // words), four in flight per thread
     char *rec = base + (slot ? (unsigned long long)*slot * stride : 0ULL);
     const CopySeg g = segs[blockIdx.y];
     char *dst = save ? rec + g.off : g.field;
     const char *src = save ? g.field : rec + g.off;
-    const unsigned long long n16 = g.bytes >> 4;
-    const unsigned long long nt = (unsigned long long)gridDim.x * blockDim.x;
+    const unsigned n16 = (unsigned)(g.bytes >> 4);
+    const unsigned nt = gridDim.x * blockDim.x;
     uint4 *d4 = reinterpret_cast<uint4 *>(dst);
     const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
-    unsigned long long q = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
     for (; q + 3 * nt < n16; q += 4 * nt) {
         const uint4 a0 = s4[q], a1 = s4[q + nt], a2 = s4[q + 2 * nt], a3 = s4[q + 3 * nt];
         d4[q] = a0;
@@ -1309,7 +1310,7 @@ __global__ void ka_list_copy(const CopySeg *segs, char *base, const long long *s
     }
     for (; q < n16; q += nt) d4[q] = s4[q];
     if (blockIdx.x == 0)
-        for (unsigned long long b = (n16 << 4) + threadIdx.x; b < g.bytes; b += blockDim.x) dst[b] = src[b];
+        for (unsigned b = (n16 << 4) + threadIdx.x; b < g.bytes; b += blockDim.x) dst[b] = src[b];
 }
 
 __global__ void ka_slot(long long *slot, long long v, int add)
