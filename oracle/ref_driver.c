@@ -115,6 +115,23 @@ int ref_init_material(void)
     return 0;
 }
 
+/*
+ * The reference builds every tracer from a stack variable whose peak pressure and temperature
+ * (mpre, mtem) it never sets (fl_data tmp_data, src/tracer.c:405-445): they start at whatever
+ * the stack held, and every peak recorded later is a MAX with that value, so two processes
+ * differ. Both start at 0 here, as the library's deck initialiser starts them.
+ */
+static void pin_tracer_peaks(sale2d_var *s)
+{
+    field_list_iterator it;
+    field_list_node *node;
+    fl_iterator_init(&it, s->tracer_list, field_list_head);
+    while ((node = fl_iterator_next(&it)) != NULL) {
+        node->data.mpre = 0.0f;
+        node->data.mtem = 0.0f;
+    }
+}
+
 /* Mirror of src/salec2d.c:76-105: first EOS call, ghost fills, PML reference state, vertex velocity, tracers. */
 int ref_init_finish(void)
 {
@@ -141,6 +158,7 @@ int ref_init_finish(void)
     g_ccl.out_vts = 1;
     g_ccl.k_out_step = 1;
     init_sale2d_tracer(&g_sale, &g_minfo);
+    pin_tracer_peaks(&g_sale);
     export_init_tracers(&g_sale, &g_minfo);
     g_stage = 3;
     return 0;
@@ -160,6 +178,7 @@ int ref_init_adopt(double damp_time)
     g_ccl.out_vts = 1;
     g_ccl.k_out_step = 1;
     init_sale2d_tracer(&g_sale, &g_minfo);
+    pin_tracer_peaks(&g_sale);
     g_stage = 3;
     return 0;
 }

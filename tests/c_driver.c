@@ -246,6 +246,17 @@ int main(int argc, char **argv)
     ccl.out_vts = 1;
     ccl.k_out_step = 1;
     init_sale2d_tracer(&sale2d, &minfo);
+    /* the reference builds every tracer from a stack variable whose peak pressure and temperature
+       it never sets (src/tracer.c:405-445); they start at 0, as in the library's own initialiser */
+    {
+        field_list_iterator it;
+        field_list_node *node;
+        fl_iterator_init(&it, sale2d.tracer_list, field_list_head);
+        while ((node = fl_iterator_next(&it)) != NULL) {
+            node->data.mpre = 0.0f;
+            node->data.mtem = 0.0f;
+        }
+    }
 
     /* ---- hand-off to the device */
     salec_run_desc run;
