@@ -201,7 +201,7 @@ __host__ __device__ __forceinline__ double ord_decode(unsigned long long u)
 
 // Second invariant of a (rr, rz, zz, theta) tensor: geometry/linear.c:188-194.
 template <class A>
-__device__ __forceinline__ A second_inv(A xx, A xy, A yy, A th)
+__host__ __device__ __forceinline__ A second_inv(A xx, A xy, A yy, A th)
 {
     return ((xx - yy) * (xx - yy) + (yy - th) * (yy - th) + (th - xx) * (th - xx)) / A(6.0) + xy * xy;
 }
@@ -434,7 +434,7 @@ __device__ __forceinline__ void material_state(const DevMat &m, double den, doub
 // Pieces of calculate_flux_mixed (src/advect.c:861-1136), templates on the scalar type (double
 // in the step, a dual number in the adjoint).
 template <class T>
-__device__ __forceinline__ T swept_volume(double xa, double ya, double xb, double yb, T dxa, T dya, T dxb, T dyb)
+__host__ __device__ __forceinline__ T swept_volume(double xa, double ya, double xb, double yb, T dxa, T dya, T dxb, T dyb)
 {
     // get_flux_volcyl (src/advect.c:1347-1354)
     const T x1 = -1.0 * dxa, y1 = -1.0 * dya, x2 = -1.0 * dxb, y2 = -1.0 * dyb;
@@ -443,7 +443,7 @@ __device__ __forceinline__ T swept_volume(double xa, double ya, double xb, doubl
 }
 
 template <class T>
-__device__ __forceinline__ T face_ratio(T p1, T p2)
+__host__ __device__ __forceinline__ T face_ratio(T p1, T p2)
 {
     // geometric_flux_ratio (src/advect.c:1312-1330)
     T a = p1, b = p2;
@@ -454,7 +454,7 @@ __device__ __forceinline__ T face_ratio(T p1, T p2)
 }
 
 template <class T>
-__device__ __forceinline__ T cut_length(T vf, T a, T b)
+__host__ __device__ __forceinline__ T cut_length(T vf, T a, T b)
 {
     // cut_length / cut_length_l / cut_length_s (src/advect.c:1356-1407)
     if (a < b) { T t = a; a = b; b = t; }
@@ -473,7 +473,7 @@ __device__ __forceinline__ T cut_length(T vf, T a, T b)
 }
 
 template <class T>
-__device__ __forceinline__ void normalise2(T &x, T &y)
+__host__ __device__ __forceinline__ void normalise2(T &x, T &y)
 {
     // vec_norm (src/geometry/linear.c:132-146)
     T len = T(0.);
@@ -517,17 +517,17 @@ __device__ __forceinline__ double algebraic_ratio(double vu, double vd, double v
 // ------------------------------------------------------------------ strength model pieces
 // Published forms as written in src/strength.c:505-570, on the arithmetic type A.
 template <class A>
-__device__ __forceinline__ A y_lundborg(A p, A y0, A fric, A ylim)
+__host__ __device__ __forceinline__ A y_lundborg(A p, A y0, A fric, A ylim)
 {
     return y0 + p * fric / (A(1) + p * fric / (ylim - y0));
 }
 template <class A>
-__device__ __forceinline__ A y_drucker(A p, A y0, A fric, A ylim)
+__host__ __device__ __forceinline__ A y_drucker(A p, A y0, A fric, A ylim)
 {
     return amin(y0 + fric * p, ylim);
 }
 template <class A>
-__device__ __forceinline__ A simon_melt(A pre, const DevMat &s)
+__host__ __device__ __forceinline__ A simon_melt(A pre, const DevMat &s)
 {
     A sol = A(s.Tmelt0) * pow(A(s.Asimon) * pre + A(1.0), A(s.Csimon));
     if (s.PolyLiq <= 0 && s.PolySol <= 0) return sol;
@@ -540,7 +540,7 @@ __device__ __forceinline__ A simon_melt(A pre, const DevMat &s)
     return amax(sol, liq);
 }
 template <class A>
-__device__ __forceinline__ A ohnaka_soft(A tem, const DevMat &s, A tmelt)
+__host__ __device__ __forceinline__ A ohnaka_soft(A tem, const DevMat &s, A tmelt)
 {
     return tanh(((tmelt + A(s.Tdelta)) / tem - A(1.0)) * A(s.Tfrac));
 }
@@ -568,7 +568,7 @@ __device__ __forceinline__ A ice_melt(A p)
 // RockStrengthT (src/strength.c:697-722) with its cohesions, frictions and limits as arguments, so
 // that the adjoint can differentiate with respect to them.
 template <class A>
-__device__ __forceinline__ A rock_strength_t(A pre, A dam, A dps, A temp, A yint0, A fint, A ylimint, A ydam0, A fdam,
+__host__ __device__ __forceinline__ A rock_strength_t(A pre, A dam, A dps, A temp, A yint0, A fint, A ylimint, A ydam0, A fdam,
                                              A ylimdam, const DevMat &s)
 {
     A yint = y_lundborg<A>(pre, yint0, fint, ylimint);
